@@ -1,0 +1,59 @@
+/*
+ * sharp_b200.h -- extensions of the B200 transform engine beyond the
+ * reference ABI.  None of these has a counterpart in the reference except
+ * where a comment names one; the reference-compatible surface is in
+ * sharp_lowlevel.h, sharp_geomhelpers.h and sharp_almhelpers.h.
+ */
+#ifndef SHARP_B200_EXT_H
+#define SHARP_B200_EXT_H
+
+#include "sharp_lowlevel.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Extra job flags, in bits the reference leaves unused (8-19). */
+enum {
+  /* Apply the transpose of the named job type:
+     Y (ALM2MAP) -> Yt, YtW (MAP2ALM) -> WY, Yt -> Y, WY -> YtW.
+     Yt is the exact adjoint of Y under <a,b> = sum_{m=0} Re(a*b)
+     + 2 sum_{m>0} Re(a*b) on a_lm and the plain dot product on maps. */
+  SHARP_ADJOINT = 1<<8,
+  /* Mixed-precision execution: FP64 recurrence, tensor-core contraction of
+     the Legendre step on split TF32 operands with FP32 accumulation
+     (flushed to FP64 per l-block).  Results are within ~1e-6 relative L2 of
+     the FP64 path. */
+  SHARP_MIXED   = 1<<9
+};
+
+/* Message of the last failed call on this thread ("" when none). */
+const char *sharp_b200_last_error(void);
+void sharp_b200_clear_error(void);
+/* 1 (default, the reference's behaviour): print the message and exit(1) on a
+   bad argument or a CUDA failure.  0: return early and keep the message for
+   sharp_b200_last_error().  The environment variable
+   SHARP_B200_ABORT_ON_ERROR=0 selects 0 at start-up. */
+void sharp_b200_set_abort_on_error(int on);
+
+/* Same job semantics as sharp_execute, but every alm/map pointer is a device
+   address on the current CUDA device and the work is enqueued on `stream`
+   (a cudaStream_t; NULL = legacy default stream) without host
+   synchronisation.  time (if non-NULL) receives the enqueue time only. */
+void sharp_b200_execute_device (sharp_jobtype type, int spin, void *alm,
+  void *map, const sharp_geom_info *geom_info, const sharp_alm_info *alm_info,
+  int ntrans, int flags, void *stream, double *time,
+  unsigned long long *opcnt);
+
+/* Drops the device tables cached for this geometry (sharp_destroy_geom_info
+   calls it). */
+void sharp_b200_forget_geometry (const sharp_geom_info *geom_info);
+
+/* Frees every cached device table and workspace of the calling process. */
+void sharp_b200_release_cache (void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

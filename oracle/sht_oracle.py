@@ -96,8 +96,8 @@ def make_geom_info(nph, ofs, stride, phi0, theta, wgt=None) -> Geometry:
 
 
 def _fapprox(a, b, eps):
-    # c_utils/c_utils.h FAPPROX: fabs(a-b) <= eps*fabs(b)
-    return abs(a - b) <= eps * abs(b)
+    # c_utils/c_utils.h:124-125 FAPPROX: fabs(a-b) < eps*fabs(b)
+    return abs(a - b) < eps * abs(b)
 
 
 def healpix_geometry(nside: int, weight=None, stride: int = 1) -> Geometry:

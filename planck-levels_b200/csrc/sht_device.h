@@ -1,0 +1,130 @@
+// Device-side plan structures and kernel launchers of the transform engine.
+//
+// Data layout in HBM (one job, FP64 internal arithmetic):
+//   * ring pairs are re-ordered by decreasing mlim (sharp_get_mlim), so the
+//     pairs that take part at a given m form the prefix [0, count_m[m]);
+//   * staged a_lm  A[(moff[m] + l - m) * ncA + comp]   (double2), scaled by the
+//     recurrence normalisation c_l (and norm_l for spin > 0); each m segment
+//     is followed by kPad zero entries so l-blocks may run past lmax;
+//   * phase       P[((m * npairs + p) * ncm + comp) * 2 + hemisphere] (double2);
+//     the two hemispheres of one (m, pair, comp) are adjacent (one 32-byte
+//     sector) so the ring FFT reads them together.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "sht_internal.h"
+
+namespace sht {
+
+constexpr int kMaxRadices = 24;
+
+// Factorisation of one complex FFT length.
+struct FftDesc {
+  int n;        // real ring length
+  int N;        // complex FFT length (n/2 for even n, n for odd n)
+  int tw;       // offset of exp(-2 pi i j/n), j<n, in the twiddle table
+  int nrad;
+  int rad[kMaxRadices];
+};
+
+// Per-geometry device tables (pairs in internal mlim order).
+struct GeomPlan {
+  const void *key = nullptr;
+  uint64_t hash = 0;
+  int lmax = -1, mmax = -1, spin = -1;
+  int npairs = 0, nphmax = 0, nmax_complex = 0;
+  std::vector<int> count_m;          // host copy, mmax+1 entries
+  std::vector<int> order;            // internal index -> reference pair index
+  std::vector<int2> synth_items;     // (m, tile) work list for synthesis
+  int synth_tile = 0;
+  // device arrays
+  double *cth = nullptr, *sth = nullptr;
+  int *mlim = nullptr, *count = nullptr;
+  int2 *items = nullptr;
+  // per ring (index 2*p + h)
+  double *phi0 = nullptr, *weight = nullptr;
+  long long *ofs = nullptr;
+  int *nph = nullptr, *stride = nullptr, *fft = nullptr;
+  FftDesc *fdesc = nullptr;
+  double2 *twiddle = nullptr;
+  long long map_lo = 0, map_hi = 0;  // pixel index extent [lo, hi)
+  bool map_covered = false;          // rings tile [lo,hi) exactly
+  ~GeomPlan();
+};
+
+// Recurrence coefficient tables for (lmax, mmax, spin).
+struct CoefPlan {
+  int lmax = -1, mmax = -1, spin = -1;
+  long long total = 0;               // table length incl. padding
+  std::vector<long long> moff;       // host copy
+  long long *d_moff = nullptr;
+  double *alpha = nullptr;           // spin 0: alpha; spin>0: a
+  double *beta = nullptr;            // spin>0: b = a * fx1
+  double *cfac = nullptr;            // c_l
+  double *seed = nullptr;            // spin 0: mfac[m]; spin>0: prefac mantissa
+  int *seed_exp = nullptr;           // spin>0: prefac exponent (base 2)
+  ~CoefPlan();
+};
+
+// a_lm addressing for one alm_info.
+struct AlmPlan {
+  const void *key = nullptr;
+  uint64_t hash = 0;
+  int lmax = 0, mmax = 0;
+  bool packed = false;
+  long long stride = 0;
+  long long lo = 0, hi = 0;          // extent in complex (or real if packed) units
+  bool covered = false;              // every element in [lo,hi) is an a_lm
+  long long *mvstart = nullptr;      // indexed by m
+  ~AlmPlan();
+};
+
+struct JobDesc {
+  int type;        // SHARP_ALM2MAP, SHARP_MAP2ALM, SHARP_ALM2MAP_DERIV1
+  int spin;
+  int nmaps, nalm;
+  int ntrans;
+  int flags;
+  int lmax, mmax;
+  bool dp;
+};
+
+// Kernel launchers (sht_legendre.cu)
+void launch_coef_tables(CoefPlan &cp, cudaStream_t st);
+void launch_legendre_synth(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
+                           const double2 *A, int ncA, int comp0, int nt,
+                           double2 *phase, int ncm, int pcomp0, cudaStream_t st);
+void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
+                          const double2 *phase, int ncm, int pcomp0, int nt,
+                          double *Aout, int ncA, int comp0, cudaStream_t st);
+
+// Ring FFT and staging launchers (sht_ring.cu)
+void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
+                     const std::vector<int> &tw_off, cudaStream_t st);
+void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, const double2 *phase, int ncm,
+                       void *const *maps_dev, int nmapptr, cudaStream_t st);
+void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, const void *const *maps_dev,
+                       int nmapptr, double2 *phase, int ncm, cudaStream_t st);
+void launch_phase2ring_direct(const JobDesc &job, const GeomPlan &gp, const double2 *phase,
+                              int ncm, void *const *maps_dev, int nmapptr, cudaStream_t st);
+void launch_ring2phase_direct(const JobDesc &job, const GeomPlan &gp,
+                              const void *const *maps_dev, int nmapptr, double2 *phase,
+                              int ncm, cudaStream_t st);
+void launch_stage_alm(const JobDesc &job, const AlmPlan &ap, const CoefPlan &cp,
+                      const double *norm_l, const void *const *alm_dev, int nalmptr,
+                      double2 *A, int ncA, cudaStream_t st);
+void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, const CoefPlan &cp,
+                        const double *norm_l, const double *Aout, int ncA,
+                        void *const *alm_dev, int nalmptr, cudaStream_t st);
+void launch_clear_maps(const JobDesc &job, const GeomPlan &gp, void *const *maps_dev,
+                       int nmapptr, cudaStream_t st);
+
+void check_cuda(cudaError_t e, const char *what, const char *file, int line);
+#define SHT_CUDA(call) ::sht::check_cuda((call), #call, __FILE__, __LINE__)
+
+}  // namespace sht

@@ -1,0 +1,650 @@
+// Job driver of the C ABI: validation with the reference's error semantics,
+// cached device plans (geometry, recurrence coefficients, a_lm layout), host
+// staging and the per-job kernel sequence.
+//
+// Reference driver: libsharp/sharp.c:762-880 (sharp_execute_job,
+// sharp_build_job_common, sharp_execute).  The reference splits ring pairs
+// into chunks and loops over m with OpenMP; here a whole job stays resident
+// in HBM and runs as: stage a_lm -> Legendre synthesis -> ring FFT (alm2map),
+// or ring FFT -> Legendre analysis -> scatter a_lm (map2alm).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "sht_device.h"
+
+namespace sht {
+
+void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  if (e == cudaSuccess) return;
+  fail(file, line, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+uint64_t fnv1a(const void *data, size_t n, uint64_t h = 1469598103934665603ull) {
+  const auto *p = static_cast<const unsigned char *>(data);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+template <typename T>
+T *dev_upload(const std::vector<T> &v, cudaStream_t st) {
+  T *d = nullptr;
+  const size_t bytes = sizeof(T) * std::max<size_t>(v.size(), 1);
+  SHT_CUDA(cudaMalloc(&d, bytes));
+  if (!v.empty())
+    SHT_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+  return d;
+}
+
+template <typename T>
+void dev_free(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+std::vector<int> factor_fft(int N) {
+  std::vector<int> r;
+  int n = N;
+  while (n % 4 == 0) { r.push_back(4); n /= 4; }
+  while (n % 2 == 0) { r.push_back(2); n /= 2; }
+  for (int p = 3; n > 1; p += 2)
+    while (n % p == 0) { r.push_back(p); n /= p; }
+  return r;
+}
+
+uint64_t hash_geom(const sharp_geom_info *g) {
+  uint64_t h = fnv1a(&g->npairs, sizeof(int));
+  h = fnv1a(&g->nphmax, sizeof(int), h);
+  if (g->npairs > 0) h = fnv1a(g->pair, sizeof(sharp_ringpair) * g->npairs, h);
+  return h;
+}
+
+uint64_t hash_alm(const sharp_alm_info *a) {
+  uint64_t h = fnv1a(&a->lmax, sizeof(int));
+  h = fnv1a(&a->nm, sizeof(int), h);
+  h = fnv1a(&a->flags, sizeof(int), h);
+  h = fnv1a(&a->stride, sizeof(ptrdiff_t), h);
+  if (a->nm > 0) {
+    h = fnv1a(a->mval, sizeof(int) * a->nm, h);
+    h = fnv1a(a->mvstart, sizeof(ptrdiff_t) * a->nm, h);
+  }
+  return h;
+}
+
+std::mutex g_cache_mutex;
+std::map<const void *, std::vector<std::unique_ptr<GeomPlan>>> g_geom_cache;
+std::vector<std::unique_ptr<CoefPlan>> g_coef_cache;
+std::map<const void *, std::unique_ptr<AlmPlan>> g_alm_cache;
+
+// ---------------------------------------------------------------------------
+// geometry plan
+// ---------------------------------------------------------------------------
+std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, int mmax, int spin,
+                                          cudaStream_t st) {
+  auto gp = std::make_unique<GeomPlan>();
+  gp->key = g;
+  gp->hash = hash_geom(g);
+  gp->lmax = lmax;
+  gp->mmax = mmax;
+  gp->spin = spin;
+  const int np = g->npairs;
+  gp->npairs = np;
+  gp->nphmax = g->nphmax;
+  std::vector<int> mlim(np);
+  for (int i = 0; i < np; ++i) mlim[i] = get_mlim(lmax, spin, g->pair[i].r1.sth, g->pair[i].r1.cth);
+  gp->order.resize(np);
+  std::iota(gp->order.begin(), gp->order.end(), 0);
+  std::stable_sort(gp->order.begin(), gp->order.end(),
+                   [&](int a, int b) { return mlim[a] > mlim[b]; });
+  // count_m[m] = number of pairs with mlim >= m (a prefix of the sorted order)
+  std::vector<int> hist(mmax + 1, 0);
+  for (int i = 0; i < np; ++i)
+    if (mlim[i] >= 0) hist[std::min(mlim[i], mmax)] += 1;
+  gp->count_m.assign(mmax + 1, 0);
+  int run = 0;
+  for (int m = mmax; m >= 0; --m) {
+    run += hist[m];
+    gp->count_m[m] = run;
+  }
+  gp->synth_tile = 256;
+  for (int m = 0; m <= mmax; ++m)
+    for (int t = 0; t * gp->synth_tile < gp->count_m[m]; ++t) gp->synth_items.push_back({m, t});
+
+  std::vector<double> cth(np), sth(np), phi0(2 * np), weight(2 * np);
+  std::vector<int> ml_sorted(np), nph(2 * np), stride(2 * np), fft(2 * np, 0);
+  std::vector<long long> ofs(2 * np);
+  std::map<int, int> len_index;
+  std::vector<FftDesc> descs;
+  long long tw_total = 0;
+  std::vector<int> tw_n, tw_off;
+  long long lo = 0, hi = 0;
+  bool first = true, unit_stride = true;
+  std::vector<std::pair<long long, long long>> spans;
+  for (int p = 0; p < np; ++p) {
+    const sharp_ringpair &pr = g->pair[gp->order[p]];
+    cth[p] = pr.r1.cth;
+    sth[p] = pr.r1.sth;
+    ml_sorted[p] = mlim[gp->order[p]];
+    for (int h = 0; h < 2; ++h) {
+      const sharp_ringinfo &r = h ? pr.r2 : pr.r1;
+      const int i = 2 * p + h;
+      const bool present = (h == 0) || r.nph > 0;
+      nph[i] = present ? r.nph : -1;
+      phi0[i] = present ? r.phi0 : 0.0;
+      weight[i] = present ? r.weight : 0.0;
+      ofs[i] = present ? r.ofs : 0;
+      stride[i] = present ? r.stride : 1;
+      if (!present || r.nph <= 0) continue;
+      auto it = len_index.find(r.nph);
+      if (it == len_index.end()) {
+        FftDesc d{};
+        d.n = r.nph;
+        d.N = (r.nph & 1) ? r.nph : r.nph / 2;
+        d.tw = int(tw_total);
+        auto rad = factor_fft(d.N);
+        SHT_REQUIRE(int(rad.size()) <= kMaxRadices, "ring length has too many factors");
+        d.nrad = int(rad.size());
+        for (int k = 0; k < d.nrad; ++k) d.rad[k] = rad[k];
+        tw_n.push_back(d.n);
+        tw_off.push_back(int(tw_total));
+        tw_total += d.n;
+        it = len_index.emplace(r.nph, int(descs.size())).first;
+        descs.push_back(d);
+        gp->nmax_complex = std::max(gp->nmax_complex, d.N);
+      }
+      fft[i] = it->second;
+      const long long a = r.ofs, b = r.ofs + (long long)(r.nph - 1) * r.stride;
+      const long long rlo = std::min(a, b), rhi = std::max(a, b) + 1;
+      if (first) { lo = rlo; hi = rhi; first = false; }
+      lo = std::min(lo, rlo);
+      hi = std::max(hi, rhi);
+      if (r.stride != 1) unit_stride = false;
+      spans.push_back({rlo, rhi});
+    }
+  }
+  SHT_REQUIRE(tw_total < (1ll << 31), "geometry too large (twiddle table)");
+  // rings tile [lo,hi) exactly -> synthesis need not pre-load the map
+  bool covered = unit_stride && !spans.empty();
+  if (covered) {
+    std::sort(spans.begin(), spans.end());
+    long long cur = lo;
+    for (auto &s : spans) {
+      if (s.first != cur) { covered = false; break; }
+      cur = s.second;
+    }
+    covered = covered && cur == hi;
+  }
+  gp->map_lo = lo;
+  gp->map_hi = hi;
+  gp->map_covered = covered;
+  const size_t smem = sizeof(double2) * 2 * (gp->nmax_complex + 2);
+  SHT_REQUIRE(smem <= 227 * 1024,
+              "ring length exceeds the shared-memory FFT limit (nph <= 14500 for even, 7250 for odd lengths)");
+
+  gp->cth = dev_upload(cth, st);
+  gp->sth = dev_upload(sth, st);
+  gp->mlim = dev_upload(ml_sorted, st);
+  gp->count = dev_upload(gp->count_m, st);
+  gp->items = dev_upload(gp->synth_items, st);
+  gp->phi0 = dev_upload(phi0, st);
+  gp->weight = dev_upload(weight, st);
+  gp->ofs = dev_upload(ofs, st);
+  gp->nph = dev_upload(nph, st);
+  gp->stride = dev_upload(stride, st);
+  gp->fft = dev_upload(fft, st);
+  gp->fdesc = dev_upload(descs, st);
+  SHT_CUDA(cudaMalloc(&gp->twiddle, sizeof(double2) * std::max<long long>(tw_total, 1)));
+  launch_twiddles(*gp, int(tw_total), tw_n, tw_off, st);
+  SHT_CUDA(cudaStreamSynchronize(st));
+  return gp;
+}
+
+GeomPlan *get_geom_plan(const sharp_geom_info *g, int lmax, int mmax, int spin, cudaStream_t st) {
+  const uint64_t h = hash_geom(g);
+  auto &vec = g_geom_cache[g];
+  for (auto &p : vec)
+    if (p->hash == h && p->lmax == lmax && p->mmax == mmax && p->spin == spin) return p.get();
+  // drop stale plans of this address (content changed)
+  vec.erase(std::remove_if(vec.begin(), vec.end(), [&](auto &p) { return p->hash != h; }),
+            vec.end());
+  if (vec.size() >= 8) vec.erase(vec.begin());
+  vec.push_back(build_geom_plan(g, lmax, mmax, spin, st));
+  return vec.back().get();
+}
+
+// ---------------------------------------------------------------------------
+// coefficient plan
+// ---------------------------------------------------------------------------
+// sqrt((2 mhi)! / ((mhi+mlo)! (mhi-mlo)!)) as mantissa * 2^exp
+// (prefactor of the spin seed, libsharp/sharp_ylmgen_c.c:97-118).
+void spin_prefactor(int lmax, int mmax, int s, std::vector<double> &mant, std::vector<int> &ex) {
+  std::vector<double> fm(2 * lmax + 1);
+  std::vector<int> fe(2 * lmax + 1);
+  fm[0] = 1.0;
+  fe[0] = 0;
+  for (int k = 1; k <= 2 * lmax; ++k) {
+    int e;
+    fm[k] = std::frexp(fm[k - 1] * std::sqrt(double(k)), &e);
+    fe[k] = fe[k - 1] + e;
+  }
+  mant.resize(mmax + 1);
+  ex.resize(mmax + 1);
+  for (int m = 0; m <= mmax; ++m) {
+    const int mhi = std::max(m, s), mlo = std::min(m, s);
+    int e;
+    double v = std::frexp(fm[2 * mhi] / fm[mhi + mlo], &e);
+    int E = e + fe[2 * mhi] - fe[mhi + mlo];
+    v = std::frexp(v / fm[mhi - mlo], &e);
+    E += e - fe[mhi - mlo];
+    mant[m] = v;
+    ex[m] = E;
+  }
+}
+
+CoefPlan *get_coef_plan(int lmax, int mmax, int spin, cudaStream_t st) {
+  for (auto &p : g_coef_cache)
+    if (p->lmax == lmax && p->mmax == mmax && p->spin == spin) return p.get();
+  auto cp = std::make_unique<CoefPlan>();
+  cp->lmax = lmax;
+  cp->mmax = mmax;
+  cp->spin = spin;
+  cp->moff.resize(mmax + 2);
+  long long off = 0;
+  for (int m = 0; m <= mmax; ++m) {
+    cp->moff[m] = off;
+    off += (lmax - m + 1) + kPad;
+  }
+  cp->moff[mmax + 1] = off;
+  cp->total = off;
+  cp->d_moff = dev_upload(cp->moff, st);
+  SHT_CUDA(cudaMalloc(&cp->alpha, sizeof(double) * off));
+  SHT_CUDA(cudaMalloc(&cp->cfac, sizeof(double) * off));
+  if (spin > 0) {
+    SHT_CUDA(cudaMalloc(&cp->beta, sizeof(double) * off));
+    std::vector<double> mant;
+    std::vector<int> ex;
+    spin_prefactor(lmax, mmax, spin, mant, ex);
+    cp->seed = dev_upload(mant, st);
+    cp->seed_exp = dev_upload(ex, st);
+  } else {
+    std::vector<double> mfac(mmax + 1);
+    mfac[0] = 0.2820947917738781434740397257803862929220;  // 1/sqrt(4 pi)
+    for (int m = 1; m <= mmax; ++m) mfac[m] = mfac[m - 1] * std::sqrt((2 * m + 1.) / (2 * m));
+    cp->seed = dev_upload(mfac, st);
+  }
+  launch_coef_tables(*cp, st);
+  SHT_CUDA(cudaStreamSynchronize(st));
+  if (g_coef_cache.size() >= 6) g_coef_cache.erase(g_coef_cache.begin());
+  g_coef_cache.push_back(std::move(cp));
+  return g_coef_cache.back().get();
+}
+
+// ---------------------------------------------------------------------------
+// a_lm plan
+// ---------------------------------------------------------------------------
+AlmPlan *get_alm_plan(const sharp_alm_info *a, int mmax, cudaStream_t st) {
+  const uint64_t h = hash_alm(a);
+  auto it = g_alm_cache.find(a);
+  if (it != g_alm_cache.end() && it->second->hash == h) return it->second.get();
+  auto ap = std::make_unique<AlmPlan>();
+  ap->key = a;
+  ap->hash = h;
+  ap->lmax = a->lmax;
+  ap->mmax = mmax;
+  ap->packed = (a->flags & SHARP_PACKED) != 0;
+  ap->stride = a->stride;
+  std::vector<long long> mv(mmax + 1, 0);
+  long long lo = 0, hi = 0, nslots = 0;
+  bool first = true;
+  for (int mi = 0; mi < a->nm; ++mi) {
+    const int m = a->mval[mi];
+    mv[m] = a->mvstart[mi];
+    for (int l = m; l <= a->lmax; l += std::max(1, a->lmax - m)) {
+      // first and last l bound the (monotone) index range of this m
+      long long i0, i1;
+      if (ap->packed && m == 0) {
+        i0 = i1 = a->mvstart[mi] + (long long)l * a->stride;
+      } else if (ap->packed) {
+        i0 = a->mvstart[mi] + 2ll * l * a->stride;
+        i1 = i0 + 1;
+      } else {
+        i0 = i1 = a->mvstart[mi] + (long long)l * a->stride;
+      }
+      const long long mn = std::min(i0, i1), mx = std::max(i0, i1) + 1;
+      if (first) { lo = mn; hi = mx; first = false; }
+      lo = std::min(lo, mn);
+      hi = std::max(hi, mx);
+      if (l == a->lmax) break;
+    }
+    nslots += (long long)(a->lmax - m + 1) * ((ap->packed && m != 0) ? 2 : 1);
+  }
+  ap->lo = lo;
+  ap->hi = hi;
+  ap->covered = (std::llabs(a->stride) == 1) && (nslots == hi - lo);
+  ap->mvstart = dev_upload(mv, st);
+  SHT_CUDA(cudaStreamSynchronize(st));
+  auto *raw = ap.get();
+  if (g_alm_cache.size() >= 64) g_alm_cache.clear();
+  g_alm_cache[a] = std::move(ap);
+  return raw;
+}
+
+// ---------------------------------------------------------------------------
+// per-device library stream
+// ---------------------------------------------------------------------------
+cudaStream_t library_stream() {
+  static std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  SHT_CUDA(cudaGetDevice(&dev));
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  SHT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  // keep freed workspace in the pool instead of returning it to the driver
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  streams[dev] = s;
+  return s;
+}
+
+struct DevBuf {
+  void *p = nullptr;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t bytes, cudaStream_t s) : st(s) {
+    if (bytes) SHT_CUDA(cudaMallocAsync(&p, bytes, s));
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  template <typename T>
+  T *as() const { return static_cast<T *>(p); }
+};
+
+double wall_now() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// ---------------------------------------------------------------------------
+// the job
+// ---------------------------------------------------------------------------
+void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
+                  const sharp_geom_info *ginfo, const sharp_alm_info *ainfo, int ntrans,
+                  int flags, bool device_ptrs, cudaStream_t user_stream, double *time,
+                  unsigned long long *opcnt) {
+  const double t0 = wall_now();
+  int type = int(type_in);
+  SHT_REQUIRE(type >= 0 && type <= 4, "bad job type");
+  SHT_REQUIRE(ginfo != nullptr && ainfo != nullptr, "null geometry or alm info");
+  SHT_REQUIRE(ntrans > 0 && ntrans <= kMaxTrans, "bad number of simultaneous transforms");
+  if (flags & SHARP_ADJOINT) {
+    // transpose of the named type (Y <-> Yt, YtW <-> WY)
+    static const int adj[5] = {SHARP_WY, SHARP_Yt, SHARP_Y, SHARP_YtW, -1};
+    SHT_REQUIRE(adj[type] >= 0, "SHARP_ADJOINT is not defined for SHARP_ALM2MAP_DERIV1");
+    type = adj[type];
+    flags &= ~int(SHARP_ADJOINT);
+  }
+  // sharp_build_job_common, libsharp/sharp.c:840-867
+  if (type == SHARP_ALM2MAP_DERIV1) spin = 1;
+  if (type == SHARP_MAP2ALM) flags |= SHARP_USE_WEIGHTS;
+  if (type == SHARP_Yt) type = SHARP_MAP2ALM;
+  if (type == SHARP_WY) {
+    type = SHARP_ALM2MAP;
+    flags |= SHARP_USE_WEIGHTS;
+  }
+  SHT_REQUIRE(spin >= 0 && spin <= ainfo->lmax, "bad spin");
+  SHT_REQUIRE(!(flags & SHARP_MIXED), "SHARP_MIXED is only available through the batched entry");
+  // all m from 0 to nm-1 exactly once (sharp_get_mmax, sharp.c:238-251)
+  const int nm = ainfo->nm;
+  {
+    std::vector<char> seen(std::max(nm, 1), 0);
+    for (int i = 0; i < nm; ++i) {
+      const int mv = ainfo->mval[i];
+      SHT_REQUIRE(mv >= 0 && mv < nm, "not all m values are present");
+      SHT_REQUIRE(!seen[mv], "duplicate m value");
+      seen[mv] = 1;
+    }
+  }
+  const int mmax = nm - 1;
+  SHT_REQUIRE(mmax <= ainfo->lmax, "incorrect l_max: must be >= m_max");
+  const bool deriv = type == SHARP_ALM2MAP_DERIV1;
+  JobDesc job{};
+  job.type = type;
+  job.spin = spin;
+  job.nmaps = (deriv || spin > 0) ? 2 : 1;
+  job.nalm = deriv ? 1 : (spin > 0 ? 2 : 1);
+  job.ntrans = ntrans;
+  job.flags = flags;
+  job.lmax = ainfo->lmax;
+  job.mmax = mmax;
+  job.dp = (flags & SHARP_DP) != 0;
+  const bool analysis = type == SHARP_MAP2ALM;
+  const bool no_fft = (flags & SHARP_NO_FFT) != 0;
+  if (no_fft)
+    for (int i = 0; i < ginfo->npairs; ++i) {
+      SHT_REQUIRE(ginfo->pair[i].r1.nph == mmax + 1, "bad ring size");
+      SHT_REQUIRE(ginfo->pair[i].r2.nph < 0 || ginfo->pair[i].r2.nph == mmax + 1, "bad ring size");
+    }
+
+  std::lock_guard<std::mutex> lk(g_cache_mutex);
+  cudaStream_t st = device_ptrs ? user_stream : library_stream();
+  GeomPlan *gp = get_geom_plan(ginfo, job.lmax, mmax, spin, st);
+  CoefPlan *cp = get_coef_plan(job.lmax, mmax, spin, st);
+  AlmPlan *ap = get_alm_plan(ainfo, mmax, st);
+
+  const int nalmptr = ntrans * job.nalm;
+  const int nmapptr = ntrans * job.nmaps;
+  const int ncA = nalmptr;
+  const int ncm = nmapptr;
+  void **alm_in = static_cast<void **>(alm);
+  void **map_in = static_cast<void **>(map);
+
+  // norm_l (libsharp/sharp_ylmgen_c.c:200-232)
+  std::vector<double> norm(job.lmax + 1, 1.0);
+  if (deriv) {
+    for (int l = 0; l <= job.lmax; ++l)
+      norm[l] = (l < 1) ? 0. : 0.5 * std::sqrt(l * (l + 1.) * (2 * l + 1.) / (4 * M_PI));
+  } else if (spin > 0) {
+    double spinsign = -1.0;
+    if (spin & 1) spinsign = -spinsign;
+    for (int l = 0; l <= job.lmax; ++l)
+      norm[l] = (l < spin) ? 0. : spinsign * 0.5 * std::sqrt((2 * l + 1) / (4 * M_PI));
+  }
+  DevBuf d_norm(sizeof(double) * norm.size(), st);
+  SHT_CUDA(cudaMemcpyAsync(d_norm.p, norm.data(), sizeof(double) * norm.size(),
+                           cudaMemcpyHostToDevice, st));
+
+  // device views of the user arrays
+  const size_t esz_map = (job.dp ? 8 : 4) * (no_fft ? 2 : 1);
+  const size_t esz_alm = (job.dp ? 8 : 4) * (ap->packed ? 1 : 2);
+  const long long map_n = gp->map_hi - gp->map_lo;
+  const long long alm_n = ap->hi - ap->lo;
+  std::vector<void *> dmap(nmapptr), dalm(nalmptr);
+  std::vector<std::unique_ptr<DevBuf>> owned;
+  long long map_lo = 0, alm_lo = 0;
+  if (device_ptrs) {
+    for (int i = 0; i < nmapptr; ++i) dmap[i] = map_in[i];
+    for (int i = 0; i < nalmptr; ++i) dalm[i] = alm_in[i];
+  } else {
+    map_lo = gp->map_lo;
+    alm_lo = ap->lo;
+    const bool load_maps = analysis || (flags & SHARP_ADD) || !gp->map_covered;
+    const bool load_alm = !analysis || (flags & SHARP_ADD) || !ap->covered;
+    for (int i = 0; i < nmapptr; ++i) {
+      owned.emplace_back(new DevBuf(esz_map * map_n, st));
+      dmap[i] = owned.back()->p;
+      if (load_maps && map_n > 0)
+        SHT_CUDA(cudaMemcpyAsync(dmap[i], static_cast<char *>(map_in[i]) + esz_map * map_lo,
+                                 esz_map * map_n, cudaMemcpyHostToDevice, st));
+    }
+    for (int i = 0; i < nalmptr; ++i) {
+      owned.emplace_back(new DevBuf(esz_alm * alm_n, st));
+      dalm[i] = owned.back()->p;
+      if (load_alm && alm_n > 0)
+        SHT_CUDA(cudaMemcpyAsync(dalm[i], static_cast<char *>(alm_in[i]) + esz_alm * alm_lo,
+                                 esz_alm * alm_n, cudaMemcpyHostToDevice, st));
+    }
+  }
+  DevBuf d_mapptr(sizeof(void *) * nmapptr, st), d_almptr(sizeof(void *) * nalmptr, st);
+  SHT_CUDA(cudaMemcpyAsync(d_mapptr.p, dmap.data(), sizeof(void *) * nmapptr,
+                           cudaMemcpyHostToDevice, st));
+  SHT_CUDA(cudaMemcpyAsync(d_almptr.p, dalm.data(), sizeof(void *) * nalmptr,
+                           cudaMemcpyHostToDevice, st));
+  GeomPlan gv = *gp;  // shallow view with the staging offset applied
+  gv.map_lo = map_lo;
+  AlmPlan av;
+  av.packed = ap->packed;
+  av.stride = ap->stride;
+  av.lo = alm_lo;
+  av.mvstart = ap->mvstart;
+
+  const size_t phase_bytes = sizeof(double2) * 2 * size_t(mmax + 1) * gp->npairs * ncm;
+  DevBuf d_phase(phase_bytes, st);
+  double2 *phase = d_phase.as<double2>();
+  const int ntmax_synth = (spin == 0 && !deriv) ? 4 : 2;
+  const int ntmax_anal = (spin == 0) ? 4 : 2;
+  auto group = [&](int left, int ntmax) {
+    int nt = 1;
+    while (nt * 2 <= ntmax && nt * 2 <= left) nt *= 2;
+    return nt;
+  };
+
+  if (!analysis) {
+    DevBuf d_A(sizeof(double2) * size_t(cp->total) * ncA, st);
+    launch_stage_alm(job, av, *cp, d_norm.as<double>(), reinterpret_cast<void *const *>(d_almptr.p),
+                     nalmptr, d_A.as<double2>(), ncA, st);
+    for (int t0 = 0; t0 < ntrans;) {
+      const int nt = group(ntrans - t0, ntmax_synth);
+      launch_legendre_synth(job, *gp, *cp, d_A.as<double2>(), ncA, t0 * job.nalm, nt, phase, ncm,
+                            t0 * job.nmaps, st);
+      t0 += nt;
+    }
+    if (no_fft)
+      launch_phase2ring_direct(job, gv, phase, ncm, reinterpret_cast<void *const *>(d_mapptr.p),
+                               nmapptr, st);
+    else
+      launch_phase2ring(job, gv, phase, ncm, reinterpret_cast<void *const *>(d_mapptr.p), nmapptr,
+                        st);
+    if (!device_ptrs && map_n > 0)
+      for (int i = 0; i < nmapptr; ++i)
+        SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(map_in[i]) + esz_map * map_lo, dmap[i],
+                                 esz_map * map_n, cudaMemcpyDeviceToHost, st));
+  } else {
+    if (no_fft)
+      launch_ring2phase_direct(job, gv, reinterpret_cast<const void *const *>(d_mapptr.p),
+                               nmapptr, phase, ncm, st);
+    else
+      launch_ring2phase(job, gv, reinterpret_cast<const void *const *>(d_mapptr.p), nmapptr, phase,
+                        ncm, st);
+    DevBuf d_Aout(sizeof(double2) * size_t(cp->total) * ncA, st);
+    SHT_CUDA(cudaMemsetAsync(d_Aout.p, 0, sizeof(double2) * size_t(cp->total) * ncA, st));
+    for (int t0 = 0; t0 < ntrans;) {
+      const int nt = group(ntrans - t0, ntmax_anal);
+      launch_legendre_anal(job, *gp, *cp, phase, ncm, t0 * job.nmaps, nt, d_Aout.as<double>(),
+                           ncA, t0 * job.nalm, st);
+      t0 += nt;
+    }
+    launch_scatter_alm(job, av, *cp, d_norm.as<double>(), d_Aout.as<double>(), ncA,
+                       reinterpret_cast<void *const *>(d_almptr.p), nalmptr, st);
+    if (!device_ptrs && alm_n > 0)
+      for (int i = 0; i < nalmptr; ++i)
+        SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(alm_in[i]) + esz_alm * alm_lo, dalm[i],
+                                 esz_alm * alm_n, cudaMemcpyDeviceToHost, st));
+  }
+  if (!device_ptrs) SHT_CUDA(cudaStreamSynchronize(st));
+  owned.clear();
+
+  if (opcnt) {
+    // per (l, m, pair) weight the reference counts (sharp_core_inc2.c:173,442,585)
+    const unsigned long long c = (spin == 0 && !deriv) ? 4 + 4ull * ntrans
+                                 : deriv ? 12 + 8ull * ntrans : 12 + 16ull * ntrans;
+    unsigned long long tot = 0;
+    for (int m = 0; m <= mmax; ++m) {
+      const int l0 = (spin == 0) ? m : std::max(m, spin);
+      if (l0 <= job.lmax) tot += (unsigned long long)gp->count_m[m] * (job.lmax - l0 + 1);
+    }
+    *opcnt = tot * c;
+  }
+  if (time) *time = wall_now() - t0;
+}
+
+void guarded(const std::function<void()> &fn) {
+  try {
+    fn();
+  } catch (const Failure &) {
+    // message already recorded; non-aborting mode returns to the caller
+  }
+}
+
+}  // namespace
+
+GeomPlan::~GeomPlan() {
+  dev_free(cth); dev_free(sth); dev_free(mlim); dev_free(count); dev_free(items);
+  dev_free(phi0); dev_free(weight); dev_free(ofs); dev_free(nph); dev_free(stride);
+  dev_free(fft); dev_free(fdesc); dev_free(twiddle);
+}
+CoefPlan::~CoefPlan() {
+  dev_free(d_moff); dev_free(alpha); dev_free(beta); dev_free(cfac); dev_free(seed);
+  dev_free(seed_exp);
+}
+AlmPlan::~AlmPlan() { dev_free(mvstart); }
+
+}  // namespace sht
+
+extern "C" {
+
+void sharp_execute(sharp_jobtype type, int spin, void *alm, void *map,
+                   const sharp_geom_info *geom_info, const sharp_alm_info *alm_info, int ntrans,
+                   int flags, double *time, unsigned long long *opcnt) {
+  sht::guarded([&] {
+    sht::execute_impl(type, spin, alm, map, geom_info, alm_info, ntrans, flags, false, nullptr,
+                      time, opcnt);
+  });
+}
+
+void sharp_b200_execute_device(sharp_jobtype type, int spin, void *alm, void *map,
+                               const sharp_geom_info *geom_info, const sharp_alm_info *alm_info,
+                               int ntrans, int flags, void *stream, double *time,
+                               unsigned long long *opcnt) {
+  sht::guarded([&] {
+    sht::execute_impl(type, spin, alm, map, geom_info, alm_info, ntrans, flags, true,
+                      static_cast<cudaStream_t>(stream), time, opcnt);
+  });
+}
+
+void sharp_b200_forget_geometry(const sharp_geom_info *info) {
+  std::lock_guard<std::mutex> lk(sht::g_cache_mutex);
+  sht::g_geom_cache.erase(info);
+}
+
+void sharp_b200_release_cache(void) {
+  std::lock_guard<std::mutex> lk(sht::g_cache_mutex);
+  sht::g_geom_cache.clear();
+  sht::g_coef_cache.clear();
+  sht::g_alm_cache.clear();
+}
+
+}  // extern "C"

@@ -1,0 +1,770 @@
+// Associated-Legendre (spin 0) and Wigner-d (spin s, first derivatives)
+// recurrences of the spherical-harmonic transform, FP64, sm_100a.
+//
+// Reference: libsharp/sharp_core_inc.c:182-293 (seeds, scaled run-up) and
+// libsharp/sharp_core_inc2.c:32-619 (synthesis/analysis kernels),
+// coefficients libsharp/sharp_ylmgen_c.c:44-198.
+//
+// Design (not a translation of the SIMD code):
+//  * one thread owns R ring pairs, lanes of a warp hold consecutive pairs, so
+//    recurrence coefficients and staged a_lm are warp-uniform broadcast loads;
+//  * the three-term recurrence is rewritten with a per-l normalisation c_l
+//    (lambda_l = c_l mu_l) so that every step is mu_{l+1} = t_l mu_l - mu_{l-1}
+//    with t_l = alpha_l x (spin 0) or a_l x -/+ b_l (spin s): 2 FP64 ops per
+//    step instead of 3; c_l is folded into the staged a_lm;
+//  * seeds sin^m(theta) etc. are formed as (mantissa, exponent) pairs; while
+//    the recurrence value is below 2^-kSwitchExp it runs scaled (exponent
+//    renormalised once per l-block, nothing accumulated), then switches to
+//    plain IEEE values.  Skipped terms are < 2^-88 of the leading ones;
+//  * analysis reduces over rings with a warp transpose-reduction and a fixed
+//    cross-warp order: no atomics, bitwise repeatable results.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "sht_device.h"
+
+namespace sht {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// (mantissa, exponent) numbers for the seeds
+// ---------------------------------------------------------------------------
+struct XD {
+  double v;  // |v| in [0.5,1) or 0
+  int e;
+};
+
+__device__ __forceinline__ XD xd_norm(double v, int e) {
+  int k;
+  double mnt = frexp(v, &k);
+  return {mnt, e + k};
+}
+
+__device__ __forceinline__ XD xd_mul(XD a, XD b) { return xd_norm(a.v * b.v, a.e + b.e); }
+
+__device__ XD xd_pow(double base, int n) {
+  XD r{1.0, 0};
+  XD b = xd_norm(base, 0);
+  while (n) {
+    if (n & 1) r = xd_mul(r, b);
+    n >>= 1;
+    if (n) b = xd_mul(b, b);
+  }
+  return xd_norm(r.v, r.e);
+}
+
+// Renormalises a scaled pair (mu_cur, mu_prev) * 2^E so that the larger one
+// lies in [0.5,1); returns false if both are zero.
+__device__ __forceinline__ bool renorm_pair(double &cur, double &prev, int &E) {
+  double big = fmax(fabs(cur), fabs(prev));
+  if (big == 0.0) return false;
+  int k;
+  frexp(big, &k);
+  cur = ldexp(cur, -k);
+  prev = ldexp(prev, -k);
+  E += k;
+  return true;
+}
+
+// Lane i ends up with sum over the warp of v[i] (recursive halving).
+__device__ __forceinline__ double warp_transpose_reduce32(double (&v)[32]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool up = (lane & s) != 0;
+#pragma unroll
+    for (int i = 0; i < s; ++i) {
+      const double send = up ? v[i] : v[i + s];
+      const double keep = up ? v[i + s] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+  return v[0];
+}
+
+// ---------------------------------------------------------------------------
+// Coefficient tables (one thread per m)
+// ---------------------------------------------------------------------------
+__global__ void coef_spin0_kernel(int lmax, int mmax, const long long *__restrict__ moff,
+                                  double *__restrict__ alpha, double *__restrict__ cfac) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m > mmax) return;
+  const long long base = moff[m];
+  const int L = lmax - m + 1;
+  // f0[l], f1[l] as libsharp/sharp_ylmgen_c.c:160-168 (root/iroot products)
+  double c_lm1 = 1.0, c_l = 1.0;  // c_{l-1}, c_l at l=m (c_{m-1} unused)
+  for (int i = 0; i < L; ++i) {
+    const int l = m + i;
+    double f0, f1;
+    if (l == m) {
+      f0 = sqrt(double(2 * m + 3));
+      f1 = 0.0;
+    } else {
+      const double tmp = sqrt(double(2 * l + 3)) * (1.0 / sqrt(double(l + 1 + m))) *
+                         (1.0 / sqrt(double(l + 1 - m)));
+      f0 = tmp * sqrt(double(2 * l + 1));
+      f1 = tmp * sqrt(double(l + m)) * sqrt(double(l - m)) * (1.0 / sqrt(double(2 * l - 1)));
+    }
+    // c_{l+1} = f1[l] c_{l-1} (l >= m+1), c_{m+1} = 1
+    const double c_lp1 = (l == m) ? 1.0 : f1 * c_lm1;
+    cfac[base + i] = c_l;
+    alpha[base + i] = (l < lmax) ? f0 * c_l / c_lp1 : 0.0;
+    c_lm1 = c_l;
+    c_l = c_lp1;
+  }
+  for (int i = L; i < L + kPad; ++i) {
+    cfac[base + i] = 0.0;
+    alpha[base + i] = 0.0;
+  }
+}
+
+__global__ void coef_spin_kernel(int lmax, int mmax, int s, const long long *__restrict__ moff,
+                                 double *__restrict__ a, double *__restrict__ b,
+                                 double *__restrict__ cfac) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m > mmax) return;
+  const long long base = moff[m];
+  const int L = lmax - m + 1;
+  const int mhi = max(m, s);
+  for (int i = 0; i < L + kPad; ++i) {
+    a[base + i] = 0.0;
+    b[base + i] = 0.0;
+    cfac[base + i] = 0.0;
+  }
+  // fx[l+1] for the step l -> l+1, libsharp/sharp_ylmgen_c.c:172-183
+  double c_lm1 = 1.0, c_l = 1.0;
+  for (int l = mhi; l <= lmax; ++l) {
+    double fx0 = 0.0, fx1 = 0.0, fx2 = 0.0;
+    if (l < lmax) {
+      const double t = sqrt(1.0 / (l + m + 1.0)) * sqrt(1.0 / (l - m + 1.0)) *
+                       sqrt(1.0 / (l + s + 1.0)) * sqrt(1.0 / (l - s + 1.0));
+      fx0 = (l + 1.0) * (2 * l + 1.0) * t;
+      fx1 = (l == 0) ? 0.0 : double(m) * s * (1.0 / l) * (1.0 / (l + 1.0));
+      const double t2 = sqrt((l + m) / (l + m + 1.0)) * sqrt((l - m) / (l - m + 1.0)) *
+                        sqrt((l + s) / (l + s + 1.0)) * sqrt((l - s) / (l - s + 1.0));
+      fx2 = (l == 0) ? 0.0 : t2 * (l + 1.0) * (1.0 / l);
+    }
+    const double c_lp1 = (l == mhi) ? 1.0 : fx2 * c_lm1;
+    const int i = l - m;
+    cfac[base + i] = c_l;
+    if (l < lmax) {
+      const double al = fx0 * c_l / c_lp1;
+      a[base + i] = al;
+      b[base + i] = al * fx1;
+    }
+    c_lm1 = c_l;
+    c_l = c_lp1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spin-0 synthesis: phase[m][p] = sum_l lambda_lm(theta_p) a_lm, split into
+// even (p1) and odd (p2) l-m; north = p1+p2, south = p1-p2.
+// ---------------------------------------------------------------------------
+template <int NT, int R>
+__global__ void __launch_bounds__(128)
+synth_spin0_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
+                   const double *__restrict__ cth, const double *__restrict__ sth,
+                   const int *__restrict__ nph_ring, const long long *__restrict__ moff,
+                   const double *__restrict__ alpha, const double *__restrict__ mfac,
+                   const double2 *__restrict__ A, int ncA, int comp0, int lmax, int npairs,
+                   double2 *__restrict__ phase, int ncm, int pcomp0) {
+  const int2 it = items[blockIdx.x];
+  const int m = it.x;
+  const int cnt = count[m];
+  const long long mo = moff[m] - m;  // table index of l is mo + l
+  const double *al = alpha + mo;
+  const double2 *Am = A + mo * ncA + comp0;
+
+  double x[R], mu0[R], mu1[R];
+  int E[R];
+  bool act[R], live[R];
+  double2 p1[R][NT], p2[R][NT];
+  const double sgn_mfac = (m & 1) ? -mfac[m] : mfac[m];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int p = it.y * (128 * R) + r * 128 + threadIdx.x;
+    const bool valid = p < cnt;
+    x[r] = valid ? cth[p] : 0.0;
+    XD sd = valid ? xd_pow(sth[p], m) : XD{0.0, 0};
+    sd = xd_norm(sd.v * sgn_mfac, sd.e);
+    mu0[r] = 0.0;
+    mu1[r] = sd.v;
+    E[r] = sd.e;
+    live[r] = valid && sd.v != 0.0;
+    act[r] = live[r] && E[r] >= -kSwitchExp;
+    if (act[r]) mu1[r] = ldexp(mu1[r], E[r]);
+#pragma unroll
+    for (int j = 0; j < NT; ++j) p1[r][j] = p2[r][j] = make_double2(0.0, 0.0);
+  }
+
+  for (int lb = m; lb <= lmax; lb += kLBlock) {
+#pragma unroll 4
+    for (int i = 0; i < kLBlock; i += 2) {
+      const int l = lb + i;
+      const double a0 = __ldg(al + l), a1 = __ldg(al + l + 1);
+      double2 A0[NT], A1[NT];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        A0[j] = __ldg(Am + (long long)l * ncA + j);
+        A1[j] = __ldg(Am + (long long)(l + 1) * ncA + j);
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double nm = fma(a0 * x[r], mu1[r], -mu0[r]);
+        const double nn = fma(a1 * x[r], nm, -mu1[r]);
+        if (act[r]) {
+#pragma unroll
+          for (int j = 0; j < NT; ++j) {
+            p1[r][j].x = fma(mu1[r], A0[j].x, p1[r][j].x);
+            p1[r][j].y = fma(mu1[r], A0[j].y, p1[r][j].y);
+            p2[r][j].x = fma(nm, A1[j].x, p2[r][j].x);
+            p2[r][j].y = fma(nm, A1[j].y, p2[r][j].y);
+          }
+        }
+        mu0[r] = nm;
+        mu1[r] = nn;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (live[r] && !act[r]) {
+        live[r] = renorm_pair(mu1[r], mu0[r], E[r]);
+        if (live[r] && E[r] >= -kSwitchExp) {
+          mu1[r] = ldexp(mu1[r], E[r]);
+          mu0[r] = ldexp(mu0[r], E[r]);
+          act[r] = true;
+        }
+      }
+    }
+  }
+
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int p = it.y * (128 * R) + r * 128 + threadIdx.x;
+    if (p >= cnt) continue;
+    const bool has_s = nph_ring[2 * p + 1] > 0;
+    double2 *dst = phase + (((long long)m * npairs + p) * ncm + pcomp0) * 2;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      dst[2 * j] = make_double2(p1[r][j].x + p2[r][j].x, p1[r][j].y + p2[r][j].y);
+      if (has_s)
+        dst[2 * j + 1] = make_double2(p1[r][j].x - p2[r][j].x, p1[r][j].y - p2[r][j].y);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spin-s synthesis (DERIV=false: E/B -> Q/U; DERIV=true: a -> d/dtheta,
+// d/dphi with spin-1 functions).  Two recurrences mu+ / mu- share a_l, b_l.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void spin_seed(double cth, double sth, int m, int s, double pre_v,
+                                          int pre_e, XD &sp, XD &sm) {
+  // libsharp/sharp_core_inc.c:223-271 and sharp_ylmgen_c.c:186-196
+  double c2 = fmax(sqrt((1.0 + cth) * 0.5), 1e-15);
+  double s2 = fmax(sqrt((1.0 - cth) * 0.5), 1e-15);
+  if (sth < 0.0) {
+    if (cth < 0.0) c2 = -c2;
+    if (cth > 0.0) s2 = -s2;
+  }
+  const int mhi = max(m, s), mlo = min(m, s);
+  int cosPow, sinPow;
+  bool preMinus_p, preMinus_m;
+  if (mhi == m) {
+    cosPow = mhi + s;
+    sinPow = mhi - s;
+    preMinus_p = preMinus_m = ((mhi - s) & 1) != 0;
+  } else {
+    cosPow = mhi + m;
+    sinPow = mhi - m;
+    preMinus_p = false;
+    preMinus_m = ((mhi + m) & 1) != 0;
+  }
+  (void)mlo;
+  const XD pre{pre_v, pre_e};
+  sp = xd_mul(xd_mul(pre, xd_pow(c2, cosPow)), xd_pow(s2, sinPow));
+  sm = xd_mul(xd_mul(pre, xd_pow(c2, sinPow)), xd_pow(s2, cosPow));
+  if (preMinus_p) sp.v = -sp.v;
+  if (preMinus_m) sm.v = -sm.v;
+  if (s & 1) sp.v = -sp.v;
+}
+
+template <int NT, int R, bool DERIV>
+__global__ void __launch_bounds__(128)
+synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
+                  const double *__restrict__ cth, const double *__restrict__ sth,
+                  const int *__restrict__ nph_ring, const long long *__restrict__ moff,
+                  const double *__restrict__ ca, const double *__restrict__ cb,
+                  const double *__restrict__ pre_v, const int *__restrict__ pre_e, int s,
+                  const double2 *__restrict__ A, int ncA, int comp0, int lmax, int npairs,
+                  double2 *__restrict__ phase, int ncm, int pcomp0) {
+  constexpr int NA = DERIV ? 1 : 2;  // staged alm components per transform
+  const int2 it = items[blockIdx.x];
+  const int m = it.x;
+  const int cnt = count[m];
+  const int mhi = max(m, s);
+  const long long mo = moff[m] - m;
+  const double *aa = ca + mo;
+  const double *bb = cb + mo;
+  const double2 *Am = A + mo * ncA + comp0;
+
+  double x[R], mp0[R], mp1[R], mm0[R], mm1[R];
+  int Ep[R], Em[R];
+  bool act[R], live[R];
+  double2 q1[R][NT], q2[R][NT], u1[R][NT], u2[R][NT];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int p = it.y * (128 * R) + r * 128 + threadIdx.x;
+    const bool valid = p < cnt;
+    XD sp{0.0, 0}, sm{0.0, 0};
+    x[r] = valid ? cth[p] : 0.0;
+    if (valid) spin_seed(x[r], sth[p], m, s, pre_v[m], pre_e[m], sp, sm);
+    mp0[r] = mm0[r] = 0.0;
+    mp1[r] = sp.v;
+    mm1[r] = sm.v;
+    Ep[r] = sp.e;
+    Em[r] = sm.e;
+    live[r] = valid && (sp.v != 0.0 || sm.v != 0.0);
+    act[r] = live[r] && max(sp.v != 0.0 ? Ep[r] : -0x3fffffff, sm.v != 0.0 ? Em[r] : -0x3fffffff) >= -kSwitchExp;
+    if (act[r]) {
+      mp1[r] = ldexp(mp1[r], Ep[r]);
+      mm1[r] = ldexp(mm1[r], Em[r]);
+    }
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+      q1[r][j] = q2[r][j] = u1[r][j] = u2[r][j] = make_double2(0.0, 0.0);
+  }
+
+  for (int lb = mhi; lb <= lmax; lb += kLBlock) {
+#pragma unroll 2
+    for (int i = 0; i < kLBlock; i += 2) {
+      const int l = lb + i;
+      const double a0 = __ldg(aa + l), b0 = __ldg(bb + l);
+      const double a1 = __ldg(aa + l + 1), b1 = __ldg(bb + l + 1);
+      double2 G0[NT], C0[NT], G1[NT], C1[NT];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        G0[j] = __ldg(Am + (long long)l * ncA + NA * j);
+        G1[j] = __ldg(Am + (long long)(l + 1) * ncA + NA * j);
+        if (!DERIV) {
+          C0[j] = __ldg(Am + (long long)l * ncA + NA * j + 1);
+          C1[j] = __ldg(Am + (long long)(l + 1) * ncA + NA * j + 1);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        // even offset from mhi: px = p1, py = p2
+        if (act[r]) {
+          const double lw = mp1[r] + mm1[r], lx = mm1[r] - mp1[r];
+#pragma unroll
+          for (int j = 0; j < NT; ++j) {
+            q1[r][j].x = fma(G0[j].x, lw, q1[r][j].x);
+            q1[r][j].y = fma(G0[j].y, lw, q1[r][j].y);
+            u2[r][j].x = fma(G0[j].y, lx, u2[r][j].x);
+            u2[r][j].y = fma(-G0[j].x, lx, u2[r][j].y);
+            if (!DERIV) {
+              u1[r][j].x = fma(C0[j].x, lw, u1[r][j].x);
+              u1[r][j].y = fma(C0[j].y, lw, u1[r][j].y);
+              q2[r][j].x = fma(-C0[j].y, lx, q2[r][j].x);
+              q2[r][j].y = fma(C0[j].x, lx, q2[r][j].y);
+            }
+          }
+        }
+        const double np_ = fma(fma(a0, x[r], -b0), mp1[r], -mp0[r]);
+        const double nm_ = fma(fma(a0, x[r], b0), mm1[r], -mm0[r]);
+        // odd offset: px = p2, py = p1
+        if (act[r]) {
+          const double lw = np_ + nm_, lx = nm_ - np_;
+#pragma unroll
+          for (int j = 0; j < NT; ++j) {
+            q2[r][j].x = fma(G1[j].x, lw, q2[r][j].x);
+            q2[r][j].y = fma(G1[j].y, lw, q2[r][j].y);
+            u1[r][j].x = fma(G1[j].y, lx, u1[r][j].x);
+            u1[r][j].y = fma(-G1[j].x, lx, u1[r][j].y);
+            if (!DERIV) {
+              u2[r][j].x = fma(C1[j].x, lw, u2[r][j].x);
+              u2[r][j].y = fma(C1[j].y, lw, u2[r][j].y);
+              q1[r][j].x = fma(-C1[j].y, lx, q1[r][j].x);
+              q1[r][j].y = fma(C1[j].x, lx, q1[r][j].y);
+            }
+          }
+        }
+        const double nnp = fma(fma(a1, x[r], -b1), np_, -mp1[r]);
+        const double nnm = fma(fma(a1, x[r], b1), nm_, -mm1[r]);
+        mp0[r] = np_;
+        mp1[r] = nnp;
+        mm0[r] = nm_;
+        mm1[r] = nnm;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (live[r] && !act[r]) {
+        const bool lp = renorm_pair(mp1[r], mp0[r], Ep[r]);
+        const bool lm = renorm_pair(mm1[r], mm0[r], Em[r]);
+        live[r] = lp || lm;
+        const int emax = max(lp ? Ep[r] : -0x3fffffff, lm ? Em[r] : -0x3fffffff);
+        if (live[r] && emax >= -kSwitchExp) {
+          mp1[r] = ldexp(mp1[r], Ep[r]);
+          mp0[r] = ldexp(mp0[r], Ep[r]);
+          mm1[r] = ldexp(mm1[r], Em[r]);
+          mm0[r] = ldexp(mm0[r], Em[r]);
+          act[r] = true;
+        }
+      }
+    }
+  }
+
+  const double flip = ((mhi - m + s) & 1) ? -1.0 : 1.0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int p = it.y * (128 * R) + r * 128 + threadIdx.x;
+    if (p >= cnt) continue;
+    const bool has_s = nph_ring[2 * p + 1] > 0;
+    double2 *dst = phase + (((long long)m * npairs + p) * ncm + pcomp0) * 2;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      dst[4 * j + 0] = make_double2(q1[r][j].x + q2[r][j].x, q1[r][j].y + q2[r][j].y);
+      dst[4 * j + 2] = make_double2(u1[r][j].x + u2[r][j].x, u1[r][j].y + u2[r][j].y);
+      if (has_s) {
+        dst[4 * j + 1] = make_double2(flip * (q1[r][j].x - q2[r][j].x),
+                                      flip * (q1[r][j].y - q2[r][j].y));
+        dst[4 * j + 3] = make_double2(flip * (u1[r][j].x - u2[r][j].x),
+                                      flip * (u1[r][j].y - u2[r][j].y));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spin-0 analysis: one CTA per m loops over tiles of 512 ring pairs;
+// a_l += sum_p lambda_l(theta_p) (N+S or N-S).  LB*VPL == 32 values per
+// l-block are reduced across the CTA and added to Aout (owned by this CTA).
+// ---------------------------------------------------------------------------
+template <int NT, int R>
+__global__ void __launch_bounds__(256)
+anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
+                  const double *__restrict__ sth, const int *__restrict__ nph_ring,
+                  const long long *__restrict__ moff, const double *__restrict__ alpha,
+                  const double *__restrict__ mfac, const double2 *__restrict__ phase, int ncm,
+                  int pcomp0, int lmax, int npairs, double *__restrict__ Aout, int ncA,
+                  int comp0) {
+  constexpr int VPL = 2 * NT;
+  constexpr int LB = 32 / VPL;
+  static_assert(LB % 2 == 0, "l-block must be even");
+  __shared__ double red[8][32];
+  const int m = blockIdx.x;
+  const int cnt = count[m];
+  const long long mo = moff[m] - m;
+  const double *al = alpha + mo;
+  const double sgn_mfac = (m & 1) ? -mfac[m] : mfac[m];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tileP = 256 * R;
+
+  for (int tb = 0; tb < cnt; tb += tileP) {
+    double x[R], mu0[R], mu1[R];
+    int E[R];
+    bool act[R], live[R];
+    double2 P1[R][NT], P2[R][NT];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int p = tb + r * 256 + threadIdx.x;
+      const bool valid = p < cnt;
+      x[r] = valid ? cth[p] : 0.0;
+      XD sd = valid ? xd_pow(sth[p], m) : XD{0.0, 0};
+      sd = xd_norm(sd.v * sgn_mfac, sd.e);
+      mu0[r] = 0.0;
+      mu1[r] = sd.v;
+      E[r] = sd.e;
+      live[r] = valid && sd.v != 0.0;
+      act[r] = live[r] && E[r] >= -kSwitchExp;
+      if (act[r]) mu1[r] = ldexp(mu1[r], E[r]);
+      const bool has_s = valid && nph_ring[2 * p + 1] > 0;
+      const double2 *src = phase + (((long long)m * npairs + (valid ? p : 0)) * ncm + pcomp0) * 2;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const double2 n = valid ? src[2 * j] : make_double2(0.0, 0.0);
+        const double2 sv = has_s ? src[2 * j + 1] : make_double2(0.0, 0.0);
+        P1[r][j] = make_double2(n.x + sv.x, n.y + sv.y);
+        P2[r][j] = make_double2(n.x - sv.x, n.y - sv.y);
+      }
+    }
+
+    for (int lb = m; lb <= lmax; lb += LB) {
+      double v[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) v[k] = 0.0;
+      bool any = false;
+#pragma unroll
+      for (int i = 0; i < LB; i += 2) {
+        const int l = lb + i;
+        const double a0 = __ldg(al + l), a1 = __ldg(al + l + 1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double nm = fma(a0 * x[r], mu1[r], -mu0[r]);
+          const double nn = fma(a1 * x[r], nm, -mu1[r]);
+          if (act[r]) {
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+              v[i * VPL + 2 * j] = fma(mu1[r], P1[r][j].x, v[i * VPL + 2 * j]);
+              v[i * VPL + 2 * j + 1] = fma(mu1[r], P1[r][j].y, v[i * VPL + 2 * j + 1]);
+              v[(i + 1) * VPL + 2 * j] = fma(nm, P2[r][j].x, v[(i + 1) * VPL + 2 * j]);
+              v[(i + 1) * VPL + 2 * j + 1] = fma(nm, P2[r][j].y, v[(i + 1) * VPL + 2 * j + 1]);
+            }
+          }
+          mu0[r] = nm;
+          mu1[r] = nn;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        any |= act[r];
+        if (live[r] && !act[r]) {
+          live[r] = renorm_pair(mu1[r], mu0[r], E[r]);
+          if (live[r] && E[r] >= -kSwitchExp) {
+            mu1[r] = ldexp(mu1[r], E[r]);
+            mu0[r] = ldexp(mu0[r], E[r]);
+            act[r] = true;
+          }
+        }
+      }
+      if (!__syncthreads_or(any)) continue;
+      const double s = warp_transpose_reduce32(v);
+      red[warp][lane] = s;
+      __syncthreads();
+      if (warp == 0) {
+        double acc = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) acc += red[w][lane];
+        const int l = lb + lane / VPL;
+        const int k = lane % VPL;
+        Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spin-s analysis (E/B from Q/U): per l, (G.re, G.im, C.re, C.im) per
+// transform.  saddstep2, libsharp/sharp_core_inc2.c:338-364.
+// ---------------------------------------------------------------------------
+template <int NT, int R>
+__global__ void __launch_bounds__(256)
+anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
+                 const double *__restrict__ sth, const int *__restrict__ nph_ring,
+                 const long long *__restrict__ moff, const double *__restrict__ ca,
+                 const double *__restrict__ cb, const double *__restrict__ pre_v,
+                 const int *__restrict__ pre_e, int s, const double2 *__restrict__ phase,
+                 int ncm, int pcomp0, int lmax, int npairs, double *__restrict__ Aout, int ncA,
+                 int comp0) {
+  constexpr int VPL = 4 * NT;
+  constexpr int LB = 32 / VPL;
+  static_assert(LB % 2 == 0, "l-block must be even");
+  __shared__ double red[8][32];
+  const int m = blockIdx.x;
+  const int cnt = count[m];
+  const int mhi = max(m, s);
+  const long long mo = moff[m] - m;
+  const double *aa = ca + mo;
+  const double *bb = cb + mo;
+  const double flip = ((mhi - m + s) & 1) ? -1.0 : 1.0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tileP = 256 * R;
+
+  for (int tb = 0; tb < cnt; tb += tileP) {
+    double x[R], mp0[R], mp1[R], mm0[R], mm1[R];
+    int Ep[R], Em[R];
+    bool act[R], live[R];
+    double2 P1q[R][NT], P1u[R][NT], P2q[R][NT], P2u[R][NT];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int p = tb + r * 256 + threadIdx.x;
+      const bool valid = p < cnt;
+      XD sp{0.0, 0}, sm{0.0, 0};
+      x[r] = valid ? cth[p] : 0.0;
+      if (valid) spin_seed(x[r], sth[p], m, s, pre_v[m], pre_e[m], sp, sm);
+      mp0[r] = mm0[r] = 0.0;
+      mp1[r] = sp.v;
+      mm1[r] = sm.v;
+      Ep[r] = sp.e;
+      Em[r] = sm.e;
+      live[r] = valid && (sp.v != 0.0 || sm.v != 0.0);
+      act[r] = live[r] && max(sp.v != 0.0 ? Ep[r] : -0x3fffffff, sm.v != 0.0 ? Em[r] : -0x3fffffff) >= -kSwitchExp;
+      if (act[r]) {
+        mp1[r] = ldexp(mp1[r], Ep[r]);
+        mm1[r] = ldexp(mm1[r], Em[r]);
+      }
+      const bool has_s = valid && nph_ring[2 * p + 1] > 0;
+      const double2 *src = phase + (((long long)m * npairs + (valid ? p : 0)) * ncm + pcomp0) * 2;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const double2 qn = valid ? src[4 * j + 0] : make_double2(0.0, 0.0);
+        const double2 un = valid ? src[4 * j + 2] : make_double2(0.0, 0.0);
+        double2 qs = has_s ? src[4 * j + 1] : make_double2(0.0, 0.0);
+        double2 us = has_s ? src[4 * j + 3] : make_double2(0.0, 0.0);
+        qs.x *= flip; qs.y *= flip; us.x *= flip; us.y *= flip;
+        P1q[r][j] = make_double2(qn.x + qs.x, qn.y + qs.y);
+        P2q[r][j] = make_double2(qn.x - qs.x, qn.y - qs.y);
+        P1u[r][j] = make_double2(un.x + us.x, un.y + us.y);
+        P2u[r][j] = make_double2(un.x - us.x, un.y - us.y);
+      }
+    }
+
+    for (int lb = mhi; lb <= lmax; lb += LB) {
+      double v[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) v[k] = 0.0;
+      bool any = false;
+#pragma unroll
+      for (int i = 0; i < LB; i += 2) {
+        const int l = lb + i;
+        const double a0 = __ldg(aa + l), b0 = __ldg(bb + l);
+        const double a1 = __ldg(aa + l + 1), b1 = __ldg(bb + l + 1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (act[r]) {  // even offset: px = p1, py = p2
+            const double lw = mp1[r] + mm1[r], lx = mm1[r] - mp1[r];
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+              double *o = v + i * VPL + 4 * j;
+              o[0] = fma(lw, P1q[r][j].x, fma(-lx, P2u[r][j].y, o[0]));
+              o[1] = fma(lw, P1q[r][j].y, fma(lx, P2u[r][j].x, o[1]));
+              o[2] = fma(lw, P1u[r][j].x, fma(lx, P2q[r][j].y, o[2]));
+              o[3] = fma(lw, P1u[r][j].y, fma(-lx, P2q[r][j].x, o[3]));
+            }
+          }
+          const double np_ = fma(fma(a0, x[r], -b0), mp1[r], -mp0[r]);
+          const double nm_ = fma(fma(a0, x[r], b0), mm1[r], -mm0[r]);
+          if (act[r]) {  // odd offset: px = p2, py = p1
+            const double lw = np_ + nm_, lx = nm_ - np_;
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+              double *o = v + (i + 1) * VPL + 4 * j;
+              o[0] = fma(lw, P2q[r][j].x, fma(-lx, P1u[r][j].y, o[0]));
+              o[1] = fma(lw, P2q[r][j].y, fma(lx, P1u[r][j].x, o[1]));
+              o[2] = fma(lw, P2u[r][j].x, fma(lx, P1q[r][j].y, o[2]));
+              o[3] = fma(lw, P2u[r][j].y, fma(-lx, P1q[r][j].x, o[3]));
+            }
+          }
+          const double nnp = fma(fma(a1, x[r], -b1), np_, -mp1[r]);
+          const double nnm = fma(fma(a1, x[r], b1), nm_, -mm1[r]);
+          mp0[r] = np_;
+          mp1[r] = nnp;
+          mm0[r] = nm_;
+          mm1[r] = nnm;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        any |= act[r];
+        if (live[r] && !act[r]) {
+          const bool lp = renorm_pair(mp1[r], mp0[r], Ep[r]);
+          const bool lm = renorm_pair(mm1[r], mm0[r], Em[r]);
+          live[r] = lp || lm;
+          const int emax = max(lp ? Ep[r] : -0x3fffffff, lm ? Em[r] : -0x3fffffff);
+          if (live[r] && emax >= -kSwitchExp) {
+            mp1[r] = ldexp(mp1[r], Ep[r]);
+            mp0[r] = ldexp(mp0[r], Ep[r]);
+            mm1[r] = ldexp(mm1[r], Em[r]);
+            mm0[r] = ldexp(mm0[r], Em[r]);
+            act[r] = true;
+          }
+        }
+      }
+      if (!__syncthreads_or(any)) continue;
+      const double sacc = warp_transpose_reduce32(v);
+      red[warp][lane] = sacc;
+      __syncthreads();
+      if (warp == 0) {
+        double acc = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) acc += red[w][lane];
+        const int l = lb + lane / VPL;
+        const int k = lane % VPL;
+        Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+void launch_coef_tables(CoefPlan &cp, cudaStream_t st) {
+  const int threads = 128;
+  const int blocks = (cp.mmax + 1 + threads - 1) / threads;
+  if (cp.spin == 0)
+    coef_spin0_kernel<<<blocks, threads, 0, st>>>(cp.lmax, cp.mmax, cp.d_moff, cp.alpha, cp.cfac);
+  else
+    coef_spin_kernel<<<blocks, threads, 0, st>>>(cp.lmax, cp.mmax, cp.spin, cp.d_moff, cp.alpha,
+                                                 cp.beta, cp.cfac);
+  SHT_CUDA(cudaGetLastError());
+}
+
+void launch_legendre_synth(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
+                           const double2 *A, int ncA, int comp0, int nt, double2 *phase,
+                           int ncm, int pcomp0, cudaStream_t st) {
+  const int nitems = int(gp.synth_items.size());
+  if (nitems == 0) return;
+  constexpr int R = 2;
+  SHT_REQUIRE(gp.synth_tile == 128 * R, "synthesis tile mismatch");
+  const bool deriv = job.type == SHARP_ALM2MAP_DERIV1;
+  if (job.spin == 0 && !deriv) {
+#define SHT_S0(NTV)                                                                           \
+  synth_spin0_kernel<NTV, R><<<nitems, 128, 0, st>>>(                                         \
+      gp.items, gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.seed, A, ncA, comp0, \
+      job.lmax, gp.npairs, phase, ncm, pcomp0)
+    if (nt == 1) SHT_S0(1);
+    else if (nt == 2) SHT_S0(2);
+    else SHT_S0(4);
+#undef SHT_S0
+  } else {
+#define SHT_SS(NTV, DV)                                                                         \
+  synth_spin_kernel<NTV, R, DV><<<nitems, 128, 0, st>>>(                                        \
+      gp.items, gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.beta, cp.seed,        \
+      cp.seed_exp, cp.spin, A, ncA, comp0, job.lmax, gp.npairs, phase, ncm, pcomp0)
+    if (deriv) {
+      if (nt == 1) SHT_SS(1, true);
+      else SHT_SS(2, true);
+    } else {
+      if (nt == 1) SHT_SS(1, false);
+      else SHT_SS(2, false);
+    }
+#undef SHT_SS
+  }
+  SHT_CUDA(cudaGetLastError());
+}
+
+void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
+                          const double2 *phase, int ncm, int pcomp0, int nt, double *Aout,
+                          int ncA, int comp0, cudaStream_t st) {
+  const int nblocks = job.mmax + 1;
+  if (job.spin == 0) {
+#define SHT_A0(NTV)                                                                       \
+  anal_spin0_kernel<NTV, 2><<<nblocks, 256, 0, st>>>(                                     \
+      gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.seed, phase, ncm, pcomp0, \
+      job.lmax, gp.npairs, Aout, ncA, comp0)
+    if (nt == 1) SHT_A0(1);
+    else if (nt == 2) SHT_A0(2);
+    else SHT_A0(4);
+#undef SHT_A0
+  } else {
+#define SHT_AS(NTV)                                                                        \
+  anal_spin_kernel<NTV, 1><<<nblocks, 256, 0, st>>>(                                       \
+      gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.beta, cp.seed, cp.seed_exp, \
+      cp.spin, phase, ncm, pcomp0, job.lmax, gp.npairs, Aout, ncA, comp0)
+    if (nt == 1) SHT_AS(1);
+    else SHT_AS(2);
+#undef SHT_AS
+  }
+  SHT_CUDA(cudaGetLastError());
+}
+
+}  // namespace sht
