@@ -52,6 +52,19 @@ void sharp_b200_forget_geometry (const sharp_geom_info *geom_info);
 /* Frees every cached device table and workspace of the calling process. */
 void sharp_b200_release_cache (void);
 
+/* Number of CUDA kernels this library has launched in the calling process. */
+unsigned long long sharp_b200_kernel_launches (void);
+
+/* Per-kernel timing with CUDA events recorded on the launching stream around
+   every kernel of the library (off by default; costs two event records per
+   launch).  on=1 starts collecting, on=0 stops and discards. */
+void sharp_b200_profile (int on);
+/* Waits for the recorded events and returns the summed milliseconds of all
+   launches of one kernel family since profiling started ("legendre_synth",
+   "legendre_anal", "ring_synth", "ring_anal", "stage_alm", "scatter_alm");
+   *launches (if non-NULL) receives their number. */
+double sharp_b200_profile_ms (const char *family, unsigned long long *launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,9 @@ struct GeomPlan {
   double2 *twiddle = nullptr;
   long long map_lo = 0, map_hi = 0;  // pixel index extent [lo, hi)
   bool map_covered = false;          // rings tile [lo,hi) exactly
+  GeomPlan() = default;
+  GeomPlan(const GeomPlan &) = delete;   // owns device memory
+  GeomPlan &operator=(const GeomPlan &) = delete;
   ~GeomPlan();
 };
 
@@ -68,6 +71,9 @@ struct CoefPlan {
   double *cfac = nullptr;            // c_l
   double *seed = nullptr;            // spin 0: mfac[m]; spin>0: prefac mantissa
   int *seed_exp = nullptr;           // spin>0: prefac exponent (base 2)
+  CoefPlan() = default;
+  CoefPlan(const CoefPlan &) = delete;
+  CoefPlan &operator=(const CoefPlan &) = delete;
   ~CoefPlan();
 };
 
@@ -81,6 +87,9 @@ struct AlmPlan {
   long long lo = 0, hi = 0;          // extent in complex (or real if packed) units
   bool covered = false;              // every element in [lo,hi) is an a_lm
   long long *mvstart = nullptr;      // indexed by m
+  AlmPlan() = default;
+  AlmPlan(const AlmPlan &) = delete;
+  AlmPlan &operator=(const AlmPlan &) = delete;
   ~AlmPlan();
 };
 
@@ -106,23 +115,43 @@ void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan
 // Ring FFT and staging launchers (sht_ring.cu)
 void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
                      const std::vector<int> &tw_off, cudaStream_t st);
-void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, const double2 *phase, int ncm,
-                       void *const *maps_dev, int nmapptr, cudaStream_t st);
-void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, const void *const *maps_dev,
-                       int nmapptr, double2 *phase, int ncm, cudaStream_t st);
-void launch_phase2ring_direct(const JobDesc &job, const GeomPlan &gp, const double2 *phase,
-                              int ncm, void *const *maps_dev, int nmapptr, cudaStream_t st);
-void launch_ring2phase_direct(const JobDesc &job, const GeomPlan &gp,
+// map_lo / alm_lo: index (in elements of the user array) that the device
+// pointers in maps_dev / alm_dev point at (0 when they are the user's own
+// device arrays, the extent start when they are staged copies).
+void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                       const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                       cudaStream_t st);
+void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                       const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
+                       cudaStream_t st);
+void launch_phase2ring_direct(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                              const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                              cudaStream_t st);
+void launch_ring2phase_direct(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                               const void *const *maps_dev, int nmapptr, double2 *phase,
                               int ncm, cudaStream_t st);
-void launch_stage_alm(const JobDesc &job, const AlmPlan &ap, const CoefPlan &cp,
-                      const double *norm_l, const void *const *alm_dev, int nalmptr,
-                      double2 *A, int ncA, cudaStream_t st);
-void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, const CoefPlan &cp,
-                        const double *norm_l, const double *Aout, int ncA,
+void launch_stage_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
+                      const CoefPlan &cp, const double *norm_l, const void *const *alm_dev,
+                      int nalmptr, double2 *A, int ncA, cudaStream_t st);
+void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
+                        const CoefPlan &cp, const double *norm_l, const double *Aout, int ncA,
                         void *const *alm_dev, int nalmptr, cudaStream_t st);
-void launch_clear_maps(const JobDesc &job, const GeomPlan &gp, void *const *maps_dev,
-                       int nmapptr, cudaStream_t st);
+
+// Launch accounting: every launcher wraps its kernel in a ProfScope, which
+// counts the launch and, when profiling is on, records CUDA events on the
+// launching stream around it.
+class ProfScope {
+ public:
+  ProfScope(const char *family, cudaStream_t st);
+  ~ProfScope();
+  ProfScope(const ProfScope &) = delete;
+  ProfScope &operator=(const ProfScope &) = delete;
+
+ private:
+  const char *family_;
+  cudaStream_t st_;
+  cudaEvent_t start_ = nullptr;
+};
 
 void check_cuda(cudaError_t e, const char *what, const char *file, int line);
 #define SHT_CUDA(call) ::sht::check_cuda((call), #call, __FILE__, __LINE__)

@@ -513,13 +513,6 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
                            cudaMemcpyHostToDevice, st));
   SHT_CUDA(cudaMemcpyAsync(d_almptr.p, dalm.data(), sizeof(void *) * nalmptr,
                            cudaMemcpyHostToDevice, st));
-  GeomPlan gv = *gp;  // shallow view with the staging offset applied
-  gv.map_lo = map_lo;
-  AlmPlan av;
-  av.packed = ap->packed;
-  av.stride = ap->stride;
-  av.lo = alm_lo;
-  av.mvstart = ap->mvstart;
 
   const size_t phase_bytes = sizeof(double2) * 2 * size_t(mmax + 1) * gp->npairs * ncm;
   DevBuf d_phase(phase_bytes, st);
@@ -534,8 +527,9 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
 
   if (!analysis) {
     DevBuf d_A(sizeof(double2) * size_t(cp->total) * ncA, st);
-    launch_stage_alm(job, av, *cp, d_norm.as<double>(), reinterpret_cast<void *const *>(d_almptr.p),
-                     nalmptr, d_A.as<double2>(), ncA, st);
+    launch_stage_alm(job, *ap, alm_lo, *cp, d_norm.as<double>(),
+                     reinterpret_cast<void *const *>(d_almptr.p), nalmptr, d_A.as<double2>(), ncA,
+                     st);
     for (int t0 = 0; t0 < ntrans;) {
       const int nt = group(ntrans - t0, ntmax_synth);
       launch_legendre_synth(job, *gp, *cp, d_A.as<double2>(), ncA, t0 * job.nalm, nt, phase, ncm,
@@ -543,22 +537,23 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
       t0 += nt;
     }
     if (no_fft)
-      launch_phase2ring_direct(job, gv, phase, ncm, reinterpret_cast<void *const *>(d_mapptr.p),
-                               nmapptr, st);
+      launch_phase2ring_direct(job, *gp, map_lo, phase, ncm,
+                               reinterpret_cast<void *const *>(d_mapptr.p), nmapptr, st);
     else
-      launch_phase2ring(job, gv, phase, ncm, reinterpret_cast<void *const *>(d_mapptr.p), nmapptr,
-                        st);
+      launch_phase2ring(job, *gp, map_lo, phase, ncm, reinterpret_cast<void *const *>(d_mapptr.p),
+                        nmapptr, st);
     if (!device_ptrs && map_n > 0)
       for (int i = 0; i < nmapptr; ++i)
         SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(map_in[i]) + esz_map * map_lo, dmap[i],
                                  esz_map * map_n, cudaMemcpyDeviceToHost, st));
   } else {
     if (no_fft)
-      launch_ring2phase_direct(job, gv, reinterpret_cast<const void *const *>(d_mapptr.p),
-                               nmapptr, phase, ncm, st);
+      launch_ring2phase_direct(job, *gp, map_lo,
+                               reinterpret_cast<const void *const *>(d_mapptr.p), nmapptr, phase,
+                               ncm, st);
     else
-      launch_ring2phase(job, gv, reinterpret_cast<const void *const *>(d_mapptr.p), nmapptr, phase,
-                        ncm, st);
+      launch_ring2phase(job, *gp, map_lo, reinterpret_cast<const void *const *>(d_mapptr.p),
+                        nmapptr, phase, ncm, st);
     DevBuf d_Aout(sizeof(double2) * size_t(cp->total) * ncA, st);
     SHT_CUDA(cudaMemsetAsync(d_Aout.p, 0, sizeof(double2) * size_t(cp->total) * ncA, st));
     for (int t0 = 0; t0 < ntrans;) {
@@ -567,7 +562,7 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
                            ncA, t0 * job.nalm, st);
       t0 += nt;
     }
-    launch_scatter_alm(job, av, *cp, d_norm.as<double>(), d_Aout.as<double>(), ncA,
+    launch_scatter_alm(job, *ap, alm_lo, *cp, d_norm.as<double>(), d_Aout.as<double>(), ncA,
                        reinterpret_cast<void *const *>(d_almptr.p), nalmptr, st);
     if (!device_ptrs && alm_n > 0)
       for (int i = 0; i < nalmptr; ++i)

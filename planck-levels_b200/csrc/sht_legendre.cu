@@ -698,6 +698,7 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
 // Launchers
 // ---------------------------------------------------------------------------
 void launch_coef_tables(CoefPlan &cp, cudaStream_t st) {
+  ProfScope ps("coef_tables", st);
   const int threads = 128;
   const int blocks = (cp.mmax + 1 + threads - 1) / threads;
   if (cp.spin == 0)
@@ -713,6 +714,7 @@ void launch_legendre_synth(const JobDesc &job, const GeomPlan &gp, const CoefPla
                            int ncm, int pcomp0, cudaStream_t st) {
   const int nitems = int(gp.synth_items.size());
   if (nitems == 0) return;
+  ProfScope ps("legendre_synth", st);
   constexpr int R = 2;
   SHT_REQUIRE(gp.synth_tile == 128 * R, "synthesis tile mismatch");
   const bool deriv = job.type == SHARP_ALM2MAP_DERIV1;
@@ -746,6 +748,7 @@ void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan
                           const double2 *phase, int ncm, int pcomp0, int nt, double *Aout,
                           int ncA, int comp0, cudaStream_t st) {
   const int nblocks = job.mmax + 1;
+  ProfScope ps("legendre_anal", st);
   if (job.spin == 0) {
 #define SHT_A0(NTV)                                                                       \
   anal_spin0_kernel<NTV, 2><<<nblocks, 256, 0, st>>>(                                     \

@@ -445,6 +445,7 @@ void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
   SHT_CUDA(cudaMemcpyAsync(d_off, tw_off.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, st));
   (void)ntw;
   dim3 grid(8, nt);
+  ProfScope ps("twiddles", st);
   twiddle_kernel<<<grid, 256, 0, st>>>(nt, d_n, d_off, gp.twiddle);
   SHT_CUDA(cudaGetLastError());
   SHT_CUDA(cudaFreeAsync(d_n, st));
@@ -453,110 +454,119 @@ void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
 
 static size_t fft_smem(const GeomPlan &gp) { return sizeof(double2) * 2 * (gp.nmax_complex + 2); }
 
-void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, const double2 *phase, int ncm,
-                       void *const *maps_dev, int nmapptr, cudaStream_t st) {
+void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                       const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                       cudaStream_t st) {
   if (gp.npairs == 0) return;
   dim3 grid(gp.npairs, nmapptr);
   const size_t sm = fft_smem(gp);
+  ProfScope ps("ring_synth", st);
   if (job.dp) {
     auto k = phase2ring_kernel<double>;
     SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
                              gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<double *const *>(maps_dev), gp.map_lo);
+                             reinterpret_cast<double *const *>(maps_dev), map_lo);
   } else {
     auto k = phase2ring_kernel<float>;
     SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
                              gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<float *const *>(maps_dev), gp.map_lo);
+                             reinterpret_cast<float *const *>(maps_dev), map_lo);
   }
   SHT_CUDA(cudaGetLastError());
 }
 
-void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, const void *const *maps_dev,
-                       int nmapptr, double2 *phase, int ncm, cudaStream_t st) {
+void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                       const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
+                       cudaStream_t st) {
   if (gp.npairs == 0) return;
   dim3 grid(gp.npairs, nmapptr);
   const size_t sm = fft_smem(gp);
+  ProfScope ps("ring_anal", st);
   if (job.dp) {
     auto k = ring2phase_kernel<double>;
     SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
                              gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<const double *const *>(maps_dev), gp.map_lo);
+                             reinterpret_cast<const double *const *>(maps_dev), map_lo);
   } else {
     auto k = ring2phase_kernel<float>;
     SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
                              gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<const float *const *>(maps_dev), gp.map_lo);
+                             reinterpret_cast<const float *const *>(maps_dev), map_lo);
   }
   SHT_CUDA(cudaGetLastError());
 }
 
-void launch_phase2ring_direct(const JobDesc &job, const GeomPlan &gp, const double2 *phase,
-                              int ncm, void *const *maps_dev, int nmapptr, cudaStream_t st) {
+void launch_phase2ring_direct(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                              const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                              cudaStream_t st) {
   if (gp.npairs == 0) return;
   dim3 grid(gp.npairs, nmapptr);
+  ProfScope ps("ring_synth", st);
   if (job.dp)
     phase2ring_direct_kernel<double2><<<grid, 128, 0, st>>>(
         gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
-        job.flags, reinterpret_cast<double2 *const *>(maps_dev), gp.map_lo);
+        job.flags, reinterpret_cast<double2 *const *>(maps_dev), map_lo);
   else
     phase2ring_direct_kernel<float2><<<grid, 128, 0, st>>>(
         gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
-        job.flags, reinterpret_cast<float2 *const *>(maps_dev), gp.map_lo);
+        job.flags, reinterpret_cast<float2 *const *>(maps_dev), map_lo);
   SHT_CUDA(cudaGetLastError());
 }
 
-void launch_ring2phase_direct(const JobDesc &job, const GeomPlan &gp,
+void launch_ring2phase_direct(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                               const void *const *maps_dev, int nmapptr, double2 *phase,
                               int ncm, cudaStream_t st) {
   if (gp.npairs == 0) return;
   dim3 grid(gp.npairs, nmapptr);
+  ProfScope ps("ring_anal", st);
   if (job.dp)
     ring2phase_direct_kernel<double2><<<grid, 128, 0, st>>>(
         gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
-        job.flags, reinterpret_cast<const double2 *const *>(maps_dev), gp.map_lo);
+        job.flags, reinterpret_cast<const double2 *const *>(maps_dev), map_lo);
   else
     ring2phase_direct_kernel<float2><<<grid, 128, 0, st>>>(
         gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
-        job.flags, reinterpret_cast<const float2 *const *>(maps_dev), gp.map_lo);
+        job.flags, reinterpret_cast<const float2 *const *>(maps_dev), map_lo);
   SHT_CUDA(cudaGetLastError());
 }
 
-void launch_stage_alm(const JobDesc &job, const AlmPlan &ap, const CoefPlan &cp,
-                      const double *norm_l, const void *const *alm_dev, int nalmptr, double2 *A,
-                      int ncA, cudaStream_t st) {
+void launch_stage_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
+                      const CoefPlan &cp, const double *norm_l, const void *const *alm_dev,
+                      int nalmptr, double2 *A, int ncA, cudaStream_t st) {
   const bool use_norm = job.spin > 0 || job.type == SHARP_ALM2MAP_DERIV1;
   const double norm_m0 = (job.flags & SHARP_REAL_HARMONICS) ? kSqrtTwo : 1.0;
   const int blocks = job.mmax + 1;
+  ProfScope ps("stage_alm", st);
   if (job.dp)
     stage_alm_kernel<double><<<blocks, 256, 0, st>>>(
-        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, ap.lo, cp.d_moff, cp.cfac, norm_l,
+        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
         use_norm, norm_m0, reinterpret_cast<const double *const *>(alm_dev), A, ncA);
   else
     stage_alm_kernel<float><<<blocks, 256, 0, st>>>(
-        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, ap.lo, cp.d_moff, cp.cfac, norm_l,
+        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
         use_norm, norm_m0, reinterpret_cast<const float *const *>(alm_dev), A, ncA);
   SHT_CUDA(cudaGetLastError());
 }
 
-void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, const CoefPlan &cp,
-                        const double *norm_l, const double *Aout, int ncA,
+void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
+                        const CoefPlan &cp, const double *norm_l, const double *Aout, int ncA,
                         void *const *alm_dev, int nalmptr, cudaStream_t st) {
   const bool use_norm = job.spin > 0 || job.type == SHARP_ALM2MAP_DERIV1;
   const double norm_m0 = (job.flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0;
   const bool add = (job.flags & SHARP_ADD) != 0;
   const int blocks = job.mmax + 1;
+  ProfScope ps("scatter_alm", st);
   if (job.dp)
     scatter_alm_kernel<double><<<blocks, 256, 0, st>>>(
-        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, ap.lo, cp.d_moff, cp.cfac, norm_l,
+        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
         use_norm, norm_m0, add, Aout, ncA, reinterpret_cast<double *const *>(alm_dev));
   else
     scatter_alm_kernel<float><<<blocks, 256, 0, st>>>(
-        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, ap.lo, cp.d_moff, cp.cfac, norm_l,
+        job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
         use_norm, norm_m0, add, Aout, ncA, reinterpret_cast<float *const *>(alm_dev));
   SHT_CUDA(cudaGetLastError());
 }
