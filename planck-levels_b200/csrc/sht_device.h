@@ -30,6 +30,9 @@ struct FftDesc {
   int tw;       // offset of exp(-2 pi i j/n), j<n, in the twiddle table
   int nrad;
   int rad[kMaxRadices];
+  int blue;     // 1: Bluestein convolution of power-of-two length M
+  int M;
+  long long bhat;  // offset of the transformed chirp (bit-reversed, /M)
 };
 
 // Per-geometry device tables (pairs in internal mlim order).
@@ -52,6 +55,13 @@ struct GeomPlan {
   int *nph = nullptr, *stride = nullptr, *fft = nullptr;
   FftDesc *fdesc = nullptr;
   double2 *twiddle = nullptr;
+  double2 *bhat = nullptr;           // Bluestein chirp transforms
+  double2 *wpow2 = nullptr;          // exp(-2 pi i j/P), j<P, P = largest M
+  int P = 2;
+  // ring FFT size classes: pairs whose largest complex FFT length is
+  // <= cls_N[c], listed at cls_pairs[cls_start[c] .. +cls_count[c])
+  std::vector<int> cls_N, cls_start, cls_count, cls_bufA, cls_bufB;
+  int *cls_pairs = nullptr;
   long long map_lo = 0, map_hi = 0;  // pixel index extent [lo, hi)
   bool map_covered = false;          // rings tile [lo,hi) exactly
   GeomPlan() = default;
@@ -115,6 +125,7 @@ void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan
 // Ring FFT and staging launchers (sht_ring.cu)
 void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
                      const std::vector<int> &tw_off, cudaStream_t st);
+void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cudaStream_t st);
 // map_lo / alm_lo: index (in elements of the user array) that the device
 // pointers in maps_dev / alm_dev point at (0 when they are the user's own
 // device arrays, the extent start when they are staged copies).

@@ -162,6 +162,17 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
         SHT_REQUIRE(int(rad.size()) <= kMaxRadices, "ring length has too many factors");
         d.nrad = int(rad.size());
         for (int k = 0; k < d.nrad; ++k) d.rad[k] = rad[k];
+        // Stockham cost ~ N * sum(generic radices); Bluestein ~ M log2 M + 2N
+        // (power-of-two convolution of length M >= 2N-1)
+        long long direct = 0;
+        for (int r : rad) direct += (r > 5) ? r : 1;
+        direct *= d.N;
+        int M = 1, lg = 0;
+        while (M < 2 * d.N - 1) { M <<= 1; ++lg; }
+        const long long blue_cost = 2ll * ((long long)M * lg + 2ll * d.N);
+        d.blue = (d.N > 16 && blue_cost < direct) ? 1 : 0;
+        d.M = d.blue ? M : 0;
+        d.bhat = 0;
         tw_n.push_back(d.n);
         tw_off.push_back(int(tw_total));
         tw_total += d.n;
@@ -180,6 +191,13 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
     }
   }
   SHT_REQUIRE(tw_total < (1ll << 31), "geometry too large (twiddle table)");
+  long long bhat_total = 0;
+  for (auto &d : descs)
+    if (d.blue) {
+      d.bhat = bhat_total;
+      bhat_total += d.M;
+      gp->P = std::max(gp->P, d.M);
+    }
   // rings tile [lo,hi) exactly -> synthesis need not pre-load the map
   bool covered = unit_stride && !spans.empty();
   if (covered) {
@@ -194,9 +212,43 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   gp->map_lo = lo;
   gp->map_hi = hi;
   gp->map_covered = covered;
-  const size_t smem = sizeof(double2) * 2 * (gp->nmax_complex + 2);
-  SHT_REQUIRE(smem <= 227 * 1024,
-              "ring length exceeds the shared-memory FFT limit (nph <= 14500 for even, 7250 for odd lengths)");
+  // FFT size classes (the last class is capped by shared memory)
+  {
+    const int bounds[4] = {256, 1024, 4096, gp->nmax_complex};
+    std::vector<std::vector<int>> lists(4);
+    for (int p = 0; p < np; ++p) {
+      int nmx = 0;
+      for (int h = 0; h < 2; ++h)
+        if (nph[2 * p + h] > 0) nmx = std::max(nmx, descs[fft[2 * p + h]].N);
+      int c = 0;
+      while (c < 3 && nmx > bounds[c]) ++c;
+      lists[c].push_back(p);
+    }
+    std::vector<int> flat;
+    for (int c = 0; c < 4; ++c) {
+      // shared memory: buffer A holds N+2 (Stockham) or M (Bluestein)
+      // entries, buffer B N+2
+      int bufA = 2, bufB = 2;
+      for (int p : lists[c])
+        for (int h = 0; h < 2; ++h)
+          if (nph[2 * p + h] > 0) {
+            const FftDesc &d = descs[fft[2 * p + h]];
+            bufA = std::max(bufA, d.blue ? std::max(d.M, d.N + 2) : d.N + 2);
+            bufB = std::max(bufB, d.N + 2);
+          }
+      gp->cls_N.push_back(std::max(bounds[c], 1));
+      gp->cls_bufA.push_back(bufA);
+      gp->cls_bufB.push_back(bufB);
+      gp->cls_start.push_back(int(flat.size()));
+      gp->cls_count.push_back(int(lists[c].size()));
+      flat.insert(flat.end(), lists[c].begin(), lists[c].end());
+      const size_t smem = sizeof(double2) * (bufA + bufB + 64 + mmax / 64 + 2);
+      SHT_REQUIRE(smem <= 227 * 1024,
+                  "ring length exceeds the shared-memory FFT limit (about 8000 pixels for "
+                  "lengths with large prime factors, 13900 otherwise)");
+    }
+    gp->cls_pairs = dev_upload(flat, st);
+  }
 
   gp->cth = dev_upload(cth, st);
   gp->sth = dev_upload(sth, st);
@@ -212,6 +264,9 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   gp->fdesc = dev_upload(descs, st);
   SHT_CUDA(cudaMalloc(&gp->twiddle, sizeof(double2) * std::max<long long>(tw_total, 1)));
   launch_twiddles(*gp, int(tw_total), tw_n, tw_off, st);
+  SHT_CUDA(cudaMalloc(&gp->bhat, sizeof(double2) * std::max<long long>(bhat_total, 1)));
+  SHT_CUDA(cudaMalloc(&gp->wpow2, sizeof(double2) * gp->P));
+  launch_bluestein_setup(*gp, descs, st);
   SHT_CUDA(cudaStreamSynchronize(st));
   return gp;
 }
@@ -599,7 +654,8 @@ void guarded(const std::function<void()> &fn) {
 GeomPlan::~GeomPlan() {
   dev_free(cth); dev_free(sth); dev_free(mlim); dev_free(count); dev_free(items);
   dev_free(phi0); dev_free(weight); dev_free(ofs); dev_free(nph); dev_free(stride);
-  dev_free(fft); dev_free(fdesc); dev_free(twiddle);
+  dev_free(fft); dev_free(fdesc); dev_free(twiddle); dev_free(cls_pairs);
+  dev_free(bhat); dev_free(wpow2);
 }
 CoefPlan::~CoefPlan() {
   dev_free(d_moff); dev_free(alpha); dev_free(beta); dev_free(cfac); dev_free(seed);

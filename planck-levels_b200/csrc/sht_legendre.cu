@@ -18,6 +18,7 @@
 //    plain IEEE values.  Skipped terms are < 2^-88 of the leading ones;
 //  * analysis reduces over rings with a warp transpose-reduction and a fixed
 //    cross-warp order: no atomics, bitwise repeatable results.
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -161,7 +162,32 @@ __global__ void coef_spin_kernel(int lmax, int mmax, int s, const long long *__r
 }
 
 // ---------------------------------------------------------------------------
-// Spin-0 synthesis: phase[m][p] = sum_l lambda_lm(theta_p) a_lm, split into
+// Phase rows: phase[((p * ncm + comp) * 2 + hemisphere) * ms + m], ms = mmax+1
+// (ring-major so the ring FFT reads and writes contiguous m runs).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ long long phase_row(int p, int ncm, int comp, int h, int ms) {
+  return ((long long)(p * ncm + comp) * 2 + h) * ms;
+}
+
+// ---------------------------------------------------------------------------
+// Coefficient staging.  Recurrence coefficients and staged a_lm are consumed
+// in chunks of kChunk l-steps.  Each chunk is copied global -> shared with
+// cp.async into one of three buffers two chunks ahead of its use, so one
+// barrier per chunk both publishes the chunk and frees the buffer the next
+// copy overwrites.  Inside a chunk all lanes read the same shared-memory
+// words (broadcast).
+// ---------------------------------------------------------------------------
+constexpr int kChunk = 32;
+
+__device__ __forceinline__ void copy8(double *dst, const double *src) {
+  __pipeline_memcpy_async(dst, src, sizeof(double));
+}
+__device__ __forceinline__ void copy16(double2 *dst, const double2 *src) {
+  __pipeline_memcpy_async(dst, src, sizeof(double2));
+}
+
+// ---------------------------------------------------------------------------
+// Spin-0 synthesis: phase_m(p) = sum_l lambda_lm(theta_p) a_lm, split into
 // even (p1) and odd (p2) l-m; north = p1+p2, south = p1-p2.
 // ---------------------------------------------------------------------------
 template <int NT, int R>
@@ -170,14 +196,29 @@ synth_spin0_kernel(const int2 *__restrict__ items, const int *__restrict__ count
                    const double *__restrict__ cth, const double *__restrict__ sth,
                    const int *__restrict__ nph_ring, const long long *__restrict__ moff,
                    const double *__restrict__ alpha, const double *__restrict__ mfac,
-                   const double2 *__restrict__ A, int ncA, int comp0, int lmax, int npairs,
-                   double2 *__restrict__ phase, int ncm, int pcomp0) {
+                   const double2 *__restrict__ A, int ncA, int comp0, int lmax,
+                   double2 *__restrict__ phase, int ncm, int pcomp0, int ms) {
+  __shared__ double s_al[3][kChunk];
+  __shared__ double2 s_A[3][kChunk * NT];
   const int2 it = items[blockIdx.x];
   const int m = it.x;
   const int cnt = count[m];
   const long long mo = moff[m] - m;  // table index of l is mo + l
   const double *al = alpha + mo;
   const double2 *Am = A + mo * ncA + comp0;
+  const int nchunks = (lmax - m + kChunk) / kChunk;
+  auto stage = [&](int ch) {
+    if (ch < nchunks) {
+      const int lc = m + ch * kChunk;
+      const int b = ch % 3;
+      for (int t = threadIdx.x; t < kChunk; t += blockDim.x) copy8(&s_al[b][t], al + lc + t);
+      for (int t = threadIdx.x; t < kChunk * NT; t += blockDim.x)
+        copy16(&s_A[b][t], Am + (long long)(lc + t / NT) * ncA + t % NT);
+    }
+    __pipeline_commit();
+  };
+  stage(0);
+  stage(1);
 
   double x[R], mu0[R], mu1[R];
   int E[R];
@@ -201,42 +242,44 @@ synth_spin0_kernel(const int2 *__restrict__ items, const int *__restrict__ count
     for (int j = 0; j < NT; ++j) p1[r][j] = p2[r][j] = make_double2(0.0, 0.0);
   }
 
-  for (int lb = m; lb <= lmax; lb += kLBlock) {
-#pragma unroll 4
-    for (int i = 0; i < kLBlock; i += 2) {
-      const int l = lb + i;
-      const double a0 = __ldg(al + l), a1 = __ldg(al + l + 1);
-      double2 A0[NT], A1[NT];
+  for (int ch = 0; ch < nchunks; ++ch) {
+    __pipeline_wait_prior(1);
+    __syncthreads();
+    stage(ch + 2);
+    const double *ca = s_al[ch % 3];
+    const double2 *cA = s_A[ch % 3];
 #pragma unroll
-      for (int j = 0; j < NT; ++j) {
-        A0[j] = __ldg(Am + (long long)l * ncA + j);
-        A1[j] = __ldg(Am + (long long)(l + 1) * ncA + j);
+    for (int sb = 0; sb < kChunk; sb += kLBlock) {
+#pragma unroll 4
+      for (int i = sb; i < sb + kLBlock; i += 2) {
+        const double a0 = ca[i], a1 = ca[i + 1];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double nm = fma(a0 * x[r], mu1[r], -mu0[r]);
+          const double nn = fma(a1 * x[r], nm, -mu1[r]);
+          if (act[r]) {
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+              const double2 A0 = cA[i * NT + j], A1 = cA[(i + 1) * NT + j];
+              p1[r][j].x = fma(mu1[r], A0.x, p1[r][j].x);
+              p1[r][j].y = fma(mu1[r], A0.y, p1[r][j].y);
+              p2[r][j].x = fma(nm, A1.x, p2[r][j].x);
+              p2[r][j].y = fma(nm, A1.y, p2[r][j].y);
+            }
+          }
+          mu0[r] = nm;
+          mu1[r] = nn;
+        }
       }
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const double nm = fma(a0 * x[r], mu1[r], -mu0[r]);
-        const double nn = fma(a1 * x[r], nm, -mu1[r]);
-        if (act[r]) {
-#pragma unroll
-          for (int j = 0; j < NT; ++j) {
-            p1[r][j].x = fma(mu1[r], A0[j].x, p1[r][j].x);
-            p1[r][j].y = fma(mu1[r], A0[j].y, p1[r][j].y);
-            p2[r][j].x = fma(nm, A1[j].x, p2[r][j].x);
-            p2[r][j].y = fma(nm, A1[j].y, p2[r][j].y);
+        if (live[r] && !act[r]) {
+          live[r] = renorm_pair(mu1[r], mu0[r], E[r]);
+          if (live[r] && E[r] >= -kSwitchExp) {
+            mu1[r] = ldexp(mu1[r], E[r]);
+            mu0[r] = ldexp(mu0[r], E[r]);
+            act[r] = true;
           }
-        }
-        mu0[r] = nm;
-        mu1[r] = nn;
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (live[r] && !act[r]) {
-        live[r] = renorm_pair(mu1[r], mu0[r], E[r]);
-        if (live[r] && E[r] >= -kSwitchExp) {
-          mu1[r] = ldexp(mu1[r], E[r]);
-          mu0[r] = ldexp(mu0[r], E[r]);
-          act[r] = true;
         }
       }
     }
@@ -247,12 +290,12 @@ synth_spin0_kernel(const int2 *__restrict__ items, const int *__restrict__ count
     const int p = it.y * (128 * R) + r * 128 + threadIdx.x;
     if (p >= cnt) continue;
     const bool has_s = nph_ring[2 * p + 1] > 0;
-    double2 *dst = phase + (((long long)m * npairs + p) * ncm + pcomp0) * 2;
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
-      dst[2 * j] = make_double2(p1[r][j].x + p2[r][j].x, p1[r][j].y + p2[r][j].y);
+      const long long row = phase_row(p, ncm, pcomp0 + j, 0, ms);
+      phase[row + m] = make_double2(p1[r][j].x + p2[r][j].x, p1[r][j].y + p2[r][j].y);
       if (has_s)
-        dst[2 * j + 1] = make_double2(p1[r][j].x - p2[r][j].x, p1[r][j].y - p2[r][j].y);
+        phase[row + ms + m] = make_double2(p1[r][j].x - p2[r][j].x, p1[r][j].y - p2[r][j].y);
     }
   }
 }
@@ -270,7 +313,7 @@ __device__ __forceinline__ void spin_seed(double cth, double sth, int m, int s, 
     if (cth < 0.0) c2 = -c2;
     if (cth > 0.0) s2 = -s2;
   }
-  const int mhi = max(m, s), mlo = min(m, s);
+  const int mhi = max(m, s);
   int cosPow, sinPow;
   bool preMinus_p, preMinus_m;
   if (mhi == m) {
@@ -283,13 +326,51 @@ __device__ __forceinline__ void spin_seed(double cth, double sth, int m, int s, 
     preMinus_p = false;
     preMinus_m = ((mhi + m) & 1) != 0;
   }
-  (void)mlo;
   const XD pre{pre_v, pre_e};
   sp = xd_mul(xd_mul(pre, xd_pow(c2, cosPow)), xd_pow(s2, sinPow));
   sm = xd_mul(xd_mul(pre, xd_pow(c2, sinPow)), xd_pow(s2, cosPow));
   if (preMinus_p) sp.v = -sp.v;
   if (preMinus_m) sm.v = -sm.v;
   if (s & 1) sp.v = -sp.v;
+}
+
+// Starts the two spin recurrences of one ring; returns whether it is live.
+__device__ __forceinline__ bool spin_start(bool valid, double x, double sth, int m, int s,
+                                           double pre_v, int pre_e, double &mp0, double &mp1,
+                                           double &mm0, double &mm1, int &Ep, int &Em,
+                                           bool &act) {
+  XD sp{0.0, 0}, sm{0.0, 0};
+  if (valid) spin_seed(x, sth, m, s, pre_v, pre_e, sp, sm);
+  mp0 = mm0 = 0.0;
+  mp1 = sp.v;
+  mm1 = sm.v;
+  Ep = sp.e;
+  Em = sm.e;
+  const bool live = valid && (sp.v != 0.0 || sm.v != 0.0);
+  const int emax = max(sp.v != 0.0 ? Ep : -0x3fffffff, sm.v != 0.0 ? Em : -0x3fffffff);
+  act = live && emax >= -kSwitchExp;
+  if (act) {
+    mp1 = ldexp(mp1, Ep);
+    mm1 = ldexp(mm1, Em);
+  }
+  return live;
+}
+
+// End-of-block bookkeeping of a ring still in the scaled (skip) regime.
+__device__ __forceinline__ void spin_renorm(bool &live, bool &act, double &mp0, double &mp1,
+                                            double &mm0, double &mm1, int &Ep, int &Em) {
+  if (!live || act) return;
+  const bool lp = renorm_pair(mp1, mp0, Ep);
+  const bool lm = renorm_pair(mm1, mm0, Em);
+  live = lp || lm;
+  const int emax = max(lp ? Ep : -0x3fffffff, lm ? Em : -0x3fffffff);
+  if (live && emax >= -kSwitchExp) {
+    mp1 = ldexp(mp1, Ep);
+    mp0 = ldexp(mp0, Ep);
+    mm1 = ldexp(mm1, Em);
+    mm0 = ldexp(mm0, Em);
+    act = true;
+  }
 }
 
 template <int NT, int R, bool DERIV>
@@ -299,9 +380,12 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
                   const int *__restrict__ nph_ring, const long long *__restrict__ moff,
                   const double *__restrict__ ca, const double *__restrict__ cb,
                   const double *__restrict__ pre_v, const int *__restrict__ pre_e, int s,
-                  const double2 *__restrict__ A, int ncA, int comp0, int lmax, int npairs,
-                  double2 *__restrict__ phase, int ncm, int pcomp0) {
+                  const double2 *__restrict__ A, int ncA, int comp0, int lmax,
+                  double2 *__restrict__ phase, int ncm, int pcomp0, int ms) {
   constexpr int NA = DERIV ? 1 : 2;  // staged alm components per transform
+  constexpr int NC = NA * NT;        // staged alm entries per l
+  __shared__ double2 s_ab[3][kChunk];      // (a_l, b_l)
+  __shared__ double2 s_A[3][kChunk * NC];
   const int2 it = items[blockIdx.x];
   const int m = it.x;
   const int cnt = count[m];
@@ -310,6 +394,22 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
   const double *aa = ca + mo;
   const double *bb = cb + mo;
   const double2 *Am = A + mo * ncA + comp0;
+  const int nchunks = (lmax - mhi + kChunk) / kChunk;
+  auto stage = [&](int ch) {
+    if (ch < nchunks) {
+      const int lc = mhi + ch * kChunk;
+      const int b = ch % 3;
+      for (int t = threadIdx.x; t < 2 * kChunk; t += blockDim.x) {
+        double *dst = reinterpret_cast<double *>(&s_ab[b][t >> 1]) + (t & 1);
+        copy8(dst, ((t & 1) ? bb : aa) + lc + (t >> 1));
+      }
+      for (int t = threadIdx.x; t < kChunk * NC; t += blockDim.x)
+        copy16(&s_A[b][t], Am + (long long)(lc + t / NC) * ncA + t % NC);
+    }
+    __pipeline_commit();
+  };
+  stage(0);
+  stage(1);
 
   double x[R], mp0[R], mp1[R], mm0[R], mm1[R];
   int Ep[R], Em[R];
@@ -319,102 +419,78 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
   for (int r = 0; r < R; ++r) {
     const int p = it.y * (128 * R) + r * 128 + threadIdx.x;
     const bool valid = p < cnt;
-    XD sp{0.0, 0}, sm{0.0, 0};
     x[r] = valid ? cth[p] : 0.0;
-    if (valid) spin_seed(x[r], sth[p], m, s, pre_v[m], pre_e[m], sp, sm);
-    mp0[r] = mm0[r] = 0.0;
-    mp1[r] = sp.v;
-    mm1[r] = sm.v;
-    Ep[r] = sp.e;
-    Em[r] = sm.e;
-    live[r] = valid && (sp.v != 0.0 || sm.v != 0.0);
-    act[r] = live[r] && max(sp.v != 0.0 ? Ep[r] : -0x3fffffff, sm.v != 0.0 ? Em[r] : -0x3fffffff) >= -kSwitchExp;
-    if (act[r]) {
-      mp1[r] = ldexp(mp1[r], Ep[r]);
-      mm1[r] = ldexp(mm1[r], Em[r]);
-    }
+    live[r] = spin_start(valid, x[r], valid ? sth[p] : 0.0, m, s, pre_v[m], pre_e[m], mp0[r],
+                         mp1[r], mm0[r], mm1[r], Ep[r], Em[r], act[r]);
 #pragma unroll
     for (int j = 0; j < NT; ++j)
       q1[r][j] = q2[r][j] = u1[r][j] = u2[r][j] = make_double2(0.0, 0.0);
   }
 
-  for (int lb = mhi; lb <= lmax; lb += kLBlock) {
+  for (int ch = 0; ch < nchunks; ++ch) {
+    __pipeline_wait_prior(1);
+    __syncthreads();
+    stage(ch + 2);
+    const double2 *cab = s_ab[ch % 3];
+    const double2 *cA = s_A[ch % 3];
+#pragma unroll
+    for (int sb = 0; sb < kChunk; sb += kLBlock) {
 #pragma unroll 2
-    for (int i = 0; i < kLBlock; i += 2) {
-      const int l = lb + i;
-      const double a0 = __ldg(aa + l), b0 = __ldg(bb + l);
-      const double a1 = __ldg(aa + l + 1), b1 = __ldg(bb + l + 1);
-      double2 G0[NT], C0[NT], G1[NT], C1[NT];
+      for (int i = sb; i < sb + kLBlock; i += 2) {
+        const double2 ab0 = cab[i], ab1 = cab[i + 1];
 #pragma unroll
-      for (int j = 0; j < NT; ++j) {
-        G0[j] = __ldg(Am + (long long)l * ncA + NA * j);
-        G1[j] = __ldg(Am + (long long)(l + 1) * ncA + NA * j);
-        if (!DERIV) {
-          C0[j] = __ldg(Am + (long long)l * ncA + NA * j + 1);
-          C1[j] = __ldg(Am + (long long)(l + 1) * ncA + NA * j + 1);
-        }
-      }
+        for (int r = 0; r < R; ++r) {
+          // even offset from mhi: px = p1, py = p2
+          if (act[r]) {
+            const double lw = mp1[r] + mm1[r], lx = mm1[r] - mp1[r];
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        // even offset from mhi: px = p1, py = p2
-        if (act[r]) {
-          const double lw = mp1[r] + mm1[r], lx = mm1[r] - mp1[r];
-#pragma unroll
-          for (int j = 0; j < NT; ++j) {
-            q1[r][j].x = fma(G0[j].x, lw, q1[r][j].x);
-            q1[r][j].y = fma(G0[j].y, lw, q1[r][j].y);
-            u2[r][j].x = fma(G0[j].y, lx, u2[r][j].x);
-            u2[r][j].y = fma(-G0[j].x, lx, u2[r][j].y);
-            if (!DERIV) {
-              u1[r][j].x = fma(C0[j].x, lw, u1[r][j].x);
-              u1[r][j].y = fma(C0[j].y, lw, u1[r][j].y);
-              q2[r][j].x = fma(-C0[j].y, lx, q2[r][j].x);
-              q2[r][j].y = fma(C0[j].x, lx, q2[r][j].y);
+            for (int j = 0; j < NT; ++j) {
+              const double2 G0 = cA[i * NC + NA * j];
+              q1[r][j].x = fma(G0.x, lw, q1[r][j].x);
+              q1[r][j].y = fma(G0.y, lw, q1[r][j].y);
+              u2[r][j].x = fma(G0.y, lx, u2[r][j].x);
+              u2[r][j].y = fma(-G0.x, lx, u2[r][j].y);
+              if (!DERIV) {
+                const double2 C0 = cA[i * NC + NA * j + 1];
+                u1[r][j].x = fma(C0.x, lw, u1[r][j].x);
+                u1[r][j].y = fma(C0.y, lw, u1[r][j].y);
+                q2[r][j].x = fma(-C0.y, lx, q2[r][j].x);
+                q2[r][j].y = fma(C0.x, lx, q2[r][j].y);
+              }
             }
           }
-        }
-        const double np_ = fma(fma(a0, x[r], -b0), mp1[r], -mp0[r]);
-        const double nm_ = fma(fma(a0, x[r], b0), mm1[r], -mm0[r]);
-        // odd offset: px = p2, py = p1
-        if (act[r]) {
-          const double lw = np_ + nm_, lx = nm_ - np_;
+          const double np_ = fma(fma(ab0.x, x[r], -ab0.y), mp1[r], -mp0[r]);
+          const double nm_ = fma(fma(ab0.x, x[r], ab0.y), mm1[r], -mm0[r]);
+          // odd offset: px = p2, py = p1
+          if (act[r]) {
+            const double lw = np_ + nm_, lx = nm_ - np_;
 #pragma unroll
-          for (int j = 0; j < NT; ++j) {
-            q2[r][j].x = fma(G1[j].x, lw, q2[r][j].x);
-            q2[r][j].y = fma(G1[j].y, lw, q2[r][j].y);
-            u1[r][j].x = fma(G1[j].y, lx, u1[r][j].x);
-            u1[r][j].y = fma(-G1[j].x, lx, u1[r][j].y);
-            if (!DERIV) {
-              u2[r][j].x = fma(C1[j].x, lw, u2[r][j].x);
-              u2[r][j].y = fma(C1[j].y, lw, u2[r][j].y);
-              q1[r][j].x = fma(-C1[j].y, lx, q1[r][j].x);
-              q1[r][j].y = fma(C1[j].x, lx, q1[r][j].y);
+            for (int j = 0; j < NT; ++j) {
+              const double2 G1 = cA[(i + 1) * NC + NA * j];
+              q2[r][j].x = fma(G1.x, lw, q2[r][j].x);
+              q2[r][j].y = fma(G1.y, lw, q2[r][j].y);
+              u1[r][j].x = fma(G1.y, lx, u1[r][j].x);
+              u1[r][j].y = fma(-G1.x, lx, u1[r][j].y);
+              if (!DERIV) {
+                const double2 C1 = cA[(i + 1) * NC + NA * j + 1];
+                u2[r][j].x = fma(C1.x, lw, u2[r][j].x);
+                u2[r][j].y = fma(C1.y, lw, u2[r][j].y);
+                q1[r][j].x = fma(-C1.y, lx, q1[r][j].x);
+                q1[r][j].y = fma(C1.x, lx, q1[r][j].y);
+              }
             }
           }
+          const double nnp = fma(fma(ab1.x, x[r], -ab1.y), np_, -mp1[r]);
+          const double nnm = fma(fma(ab1.x, x[r], ab1.y), nm_, -mm1[r]);
+          mp0[r] = np_;
+          mp1[r] = nnp;
+          mm0[r] = nm_;
+          mm1[r] = nnm;
         }
-        const double nnp = fma(fma(a1, x[r], -b1), np_, -mp1[r]);
-        const double nnm = fma(fma(a1, x[r], b1), nm_, -mm1[r]);
-        mp0[r] = np_;
-        mp1[r] = nnp;
-        mm0[r] = nm_;
-        mm1[r] = nnm;
       }
-    }
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (live[r] && !act[r]) {
-        const bool lp = renorm_pair(mp1[r], mp0[r], Ep[r]);
-        const bool lm = renorm_pair(mm1[r], mm0[r], Em[r]);
-        live[r] = lp || lm;
-        const int emax = max(lp ? Ep[r] : -0x3fffffff, lm ? Em[r] : -0x3fffffff);
-        if (live[r] && emax >= -kSwitchExp) {
-          mp1[r] = ldexp(mp1[r], Ep[r]);
-          mp0[r] = ldexp(mp0[r], Ep[r]);
-          mm1[r] = ldexp(mm1[r], Em[r]);
-          mm0[r] = ldexp(mm0[r], Em[r]);
-          act[r] = true;
-        }
-      }
+      for (int r = 0; r < R; ++r)
+        spin_renorm(live[r], act[r], mp0[r], mp1[r], mm0[r], mm1[r], Ep[r], Em[r]);
     }
   }
 
@@ -424,54 +500,69 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
     const int p = it.y * (128 * R) + r * 128 + threadIdx.x;
     if (p >= cnt) continue;
     const bool has_s = nph_ring[2 * p + 1] > 0;
-    double2 *dst = phase + (((long long)m * npairs + p) * ncm + pcomp0) * 2;
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
-      dst[4 * j + 0] = make_double2(q1[r][j].x + q2[r][j].x, q1[r][j].y + q2[r][j].y);
-      dst[4 * j + 2] = make_double2(u1[r][j].x + u2[r][j].x, u1[r][j].y + u2[r][j].y);
+      const long long rq = phase_row(p, ncm, pcomp0 + 2 * j, 0, ms);
+      const long long ru = phase_row(p, ncm, pcomp0 + 2 * j + 1, 0, ms);
+      phase[rq + m] = make_double2(q1[r][j].x + q2[r][j].x, q1[r][j].y + q2[r][j].y);
+      phase[ru + m] = make_double2(u1[r][j].x + u2[r][j].x, u1[r][j].y + u2[r][j].y);
       if (has_s) {
-        dst[4 * j + 1] = make_double2(flip * (q1[r][j].x - q2[r][j].x),
-                                      flip * (q1[r][j].y - q2[r][j].y));
-        dst[4 * j + 3] = make_double2(flip * (u1[r][j].x - u2[r][j].x),
-                                      flip * (u1[r][j].y - u2[r][j].y));
+        phase[rq + ms + m] = make_double2(flip * (q1[r][j].x - q2[r][j].x),
+                                          flip * (q1[r][j].y - q2[r][j].y));
+        phase[ru + ms + m] = make_double2(flip * (u1[r][j].x - u2[r][j].x),
+                                          flip * (u1[r][j].y - u2[r][j].y));
       }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Spin-0 analysis: one CTA per m loops over tiles of 512 ring pairs;
-// a_l += sum_p lambda_l(theta_p) (N+S or N-S).  LB*VPL == 32 values per
-// l-block are reduced across the CTA and added to Aout (owned by this CTA).
+// Analysis.  One CTA of 128 threads per m loops over tiles of 128*R ring
+// pairs.  Per l-block every lane accumulates LB*VPL == 32 partial sums over
+// its R rings; a warp transpose-reduction leaves one sum per lane, the four
+// warps are combined in a fixed order and added to Aout (owned by this CTA).
+// Coefficients arrive through the shared-memory chunk pipeline; besides its
+// barrier there is one barrier per l-block (double-buffered reduction
+// scratch).
 // ---------------------------------------------------------------------------
 template <int NT, int R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
 anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
                   const double *__restrict__ sth, const int *__restrict__ nph_ring,
                   const long long *__restrict__ moff, const double *__restrict__ alpha,
                   const double *__restrict__ mfac, const double2 *__restrict__ phase, int ncm,
-                  int pcomp0, int lmax, int npairs, double *__restrict__ Aout, int ncA,
+                  int pcomp0, int lmax, int ms, double *__restrict__ Aout, int ncA,
                   int comp0) {
   constexpr int VPL = 2 * NT;
   constexpr int LB = 32 / VPL;
-  static_assert(LB % 2 == 0, "l-block must be even");
-  __shared__ double red[8][32];
+  static_assert(LB % 2 == 0 && kChunk % LB == 0, "l-block must be even and divide a chunk");
+  __shared__ double red[2][4][32];
+  __shared__ double s_al[3][kChunk];
   const int m = blockIdx.x;
   const int cnt = count[m];
   const long long mo = moff[m] - m;
   const double *al = alpha + mo;
   const double sgn_mfac = (m & 1) ? -mfac[m] : mfac[m];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tileP = 256 * R;
+  const int nchunks = (lmax - m + kChunk) / kChunk;
+  auto stage = [&](int ch) {
+    if (ch < nchunks)
+      for (int t = threadIdx.x; t < kChunk; t += blockDim.x)
+        copy8(&s_al[ch % 3][t], al + m + ch * kChunk + t);
+    __pipeline_commit();
+  };
+  int buf = 0;
 
-  for (int tb = 0; tb < cnt; tb += tileP) {
+  for (int tb = 0; tb < cnt; tb += 128 * R) {
+    stage(0);
+    stage(1);
     double x[R], mu0[R], mu1[R];
     int E[R];
     bool act[R], live[R];
     double2 P1[R][NT], P2[R][NT];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int p = tb + r * 256 + threadIdx.x;
+      const int p = tb + r * 128 + threadIdx.x;
       const bool valid = p < cnt;
       x[r] = valid ? cth[p] : 0.0;
       XD sd = valid ? xd_pow(sth[p], m) : XD{0.0, 0};
@@ -483,88 +574,93 @@ anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       act[r] = live[r] && E[r] >= -kSwitchExp;
       if (act[r]) mu1[r] = ldexp(mu1[r], E[r]);
       const bool has_s = valid && nph_ring[2 * p + 1] > 0;
-      const double2 *src = phase + (((long long)m * npairs + (valid ? p : 0)) * ncm + pcomp0) * 2;
 #pragma unroll
       for (int j = 0; j < NT; ++j) {
-        const double2 n = valid ? src[2 * j] : make_double2(0.0, 0.0);
-        const double2 sv = has_s ? src[2 * j + 1] : make_double2(0.0, 0.0);
+        const long long row = phase_row(valid ? p : 0, ncm, pcomp0 + j, 0, ms);
+        const double2 n = valid ? phase[row + m] : make_double2(0.0, 0.0);
+        const double2 sv = has_s ? phase[row + ms + m] : make_double2(0.0, 0.0);
         P1[r][j] = make_double2(n.x + sv.x, n.y + sv.y);
         P2[r][j] = make_double2(n.x - sv.x, n.y - sv.y);
       }
     }
 
-    for (int lb = m; lb <= lmax; lb += LB) {
-      double v[32];
+    for (int ch = 0; ch < nchunks; ++ch) {
+      __pipeline_wait_prior(1);
+      __syncthreads();
+      stage(ch + 2);
+      const double *ca = s_al[ch % 3];
+#pragma unroll 1
+      for (int sb = 0; sb < kChunk; sb += LB) {
+        double v[32];
 #pragma unroll
-      for (int k = 0; k < 32; ++k) v[k] = 0.0;
-      bool any = false;
+        for (int k = 0; k < 32; ++k) v[k] = 0.0;
 #pragma unroll
-      for (int i = 0; i < LB; i += 2) {
-        const int l = lb + i;
-        const double a0 = __ldg(al + l), a1 = __ldg(al + l + 1);
+        for (int i = 0; i < LB; i += 2) {
+          const double a0 = ca[sb + i], a1 = ca[sb + i + 1];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const double nm = fma(a0 * x[r], mu1[r], -mu0[r]);
+            const double nn = fma(a1 * x[r], nm, -mu1[r]);
+            if (act[r]) {
+#pragma unroll
+              for (int j = 0; j < NT; ++j) {
+                v[i * VPL + 2 * j] = fma(mu1[r], P1[r][j].x, v[i * VPL + 2 * j]);
+                v[i * VPL + 2 * j + 1] = fma(mu1[r], P1[r][j].y, v[i * VPL + 2 * j + 1]);
+                v[(i + 1) * VPL + 2 * j] = fma(nm, P2[r][j].x, v[(i + 1) * VPL + 2 * j]);
+                v[(i + 1) * VPL + 2 * j + 1] =
+                    fma(nm, P2[r][j].y, v[(i + 1) * VPL + 2 * j + 1]);
+              }
+            }
+            mu0[r] = nm;
+            mu1[r] = nn;
+          }
+        }
+        bool any = false;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const double nm = fma(a0 * x[r], mu1[r], -mu0[r]);
-          const double nn = fma(a1 * x[r], nm, -mu1[r]);
-          if (act[r]) {
-#pragma unroll
-            for (int j = 0; j < NT; ++j) {
-              v[i * VPL + 2 * j] = fma(mu1[r], P1[r][j].x, v[i * VPL + 2 * j]);
-              v[i * VPL + 2 * j + 1] = fma(mu1[r], P1[r][j].y, v[i * VPL + 2 * j + 1]);
-              v[(i + 1) * VPL + 2 * j] = fma(nm, P2[r][j].x, v[(i + 1) * VPL + 2 * j]);
-              v[(i + 1) * VPL + 2 * j + 1] = fma(nm, P2[r][j].y, v[(i + 1) * VPL + 2 * j + 1]);
+          any |= act[r];
+          if (live[r] && !act[r] && ((sb + LB) % kLBlock) == 0) {
+            live[r] = renorm_pair(mu1[r], mu0[r], E[r]);
+            if (live[r] && E[r] >= -kSwitchExp) {
+              mu1[r] = ldexp(mu1[r], E[r]);
+              mu0[r] = ldexp(mu0[r], E[r]);
+              act[r] = true;
             }
           }
-          mu0[r] = nm;
-          mu1[r] = nn;
         }
-      }
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        any |= act[r];
-        if (live[r] && !act[r]) {
-          live[r] = renorm_pair(mu1[r], mu0[r], E[r]);
-          if (live[r] && E[r] >= -kSwitchExp) {
-            mu1[r] = ldexp(mu1[r], E[r]);
-            mu0[r] = ldexp(mu0[r], E[r]);
-            act[r] = true;
-          }
+        any = __any_sync(0xffffffffu, any);
+        red[buf][warp][lane] = any ? warp_transpose_reduce32(v) : 0.0;
+        if (__syncthreads_or(any) && warp == 0) {
+          const double acc = (red[buf][0][lane] + red[buf][1][lane]) +
+                             (red[buf][2][lane] + red[buf][3][lane]);
+          const int l = m + ch * kChunk + sb + lane / VPL;
+          const int k = lane % VPL;
+          Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
         }
+        buf ^= 1;
       }
-      if (!__syncthreads_or(any)) continue;
-      const double s = warp_transpose_reduce32(v);
-      red[warp][lane] = s;
-      __syncthreads();
-      if (warp == 0) {
-        double acc = 0.0;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) acc += red[w][lane];
-        const int l = lb + lane / VPL;
-        const int k = lane % VPL;
-        Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
-      }
-      __syncthreads();
     }
+    __pipeline_wait_prior(0);
+    __syncthreads();
   }
 }
 
-// ---------------------------------------------------------------------------
 // Spin-s analysis (E/B from Q/U): per l, (G.re, G.im, C.re, C.im) per
 // transform.  saddstep2, libsharp/sharp_core_inc2.c:338-364.
-// ---------------------------------------------------------------------------
 template <int NT, int R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
 anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
                  const double *__restrict__ sth, const int *__restrict__ nph_ring,
                  const long long *__restrict__ moff, const double *__restrict__ ca,
                  const double *__restrict__ cb, const double *__restrict__ pre_v,
                  const int *__restrict__ pre_e, int s, const double2 *__restrict__ phase,
-                 int ncm, int pcomp0, int lmax, int npairs, double *__restrict__ Aout, int ncA,
+                 int ncm, int pcomp0, int lmax, int ms, double *__restrict__ Aout, int ncA,
                  int comp0) {
   constexpr int VPL = 4 * NT;
   constexpr int LB = 32 / VPL;
-  static_assert(LB % 2 == 0, "l-block must be even");
-  __shared__ double red[8][32];
+  static_assert(LB % 2 == 0 && kChunk % LB == 0, "l-block must be even and divide a chunk");
+  __shared__ double red[2][4][32];
+  __shared__ double2 s_ab[3][kChunk];
   const int m = blockIdx.x;
   const int cnt = count[m];
   const int mhi = max(m, s);
@@ -573,39 +669,40 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
   const double *bb = cb + mo;
   const double flip = ((mhi - m + s) & 1) ? -1.0 : 1.0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tileP = 256 * R;
+  const int nchunks = (lmax - mhi + kChunk) / kChunk;
+  auto stage = [&](int ch) {
+    if (ch < nchunks)
+      for (int t = threadIdx.x; t < 2 * kChunk; t += blockDim.x) {
+        double *dst = reinterpret_cast<double *>(&s_ab[ch % 3][t >> 1]) + (t & 1);
+        copy8(dst, ((t & 1) ? bb : aa) + mhi + ch * kChunk + (t >> 1));
+      }
+    __pipeline_commit();
+  };
+  int buf = 0;
 
-  for (int tb = 0; tb < cnt; tb += tileP) {
+  for (int tb = 0; tb < cnt; tb += 128 * R) {
+    stage(0);
+    stage(1);
     double x[R], mp0[R], mp1[R], mm0[R], mm1[R];
     int Ep[R], Em[R];
     bool act[R], live[R];
     double2 P1q[R][NT], P1u[R][NT], P2q[R][NT], P2u[R][NT];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int p = tb + r * 256 + threadIdx.x;
+      const int p = tb + r * 128 + threadIdx.x;
       const bool valid = p < cnt;
-      XD sp{0.0, 0}, sm{0.0, 0};
       x[r] = valid ? cth[p] : 0.0;
-      if (valid) spin_seed(x[r], sth[p], m, s, pre_v[m], pre_e[m], sp, sm);
-      mp0[r] = mm0[r] = 0.0;
-      mp1[r] = sp.v;
-      mm1[r] = sm.v;
-      Ep[r] = sp.e;
-      Em[r] = sm.e;
-      live[r] = valid && (sp.v != 0.0 || sm.v != 0.0);
-      act[r] = live[r] && max(sp.v != 0.0 ? Ep[r] : -0x3fffffff, sm.v != 0.0 ? Em[r] : -0x3fffffff) >= -kSwitchExp;
-      if (act[r]) {
-        mp1[r] = ldexp(mp1[r], Ep[r]);
-        mm1[r] = ldexp(mm1[r], Em[r]);
-      }
+      live[r] = spin_start(valid, x[r], valid ? sth[p] : 0.0, m, s, pre_v[m], pre_e[m],
+                           mp0[r], mp1[r], mm0[r], mm1[r], Ep[r], Em[r], act[r]);
       const bool has_s = valid && nph_ring[2 * p + 1] > 0;
-      const double2 *src = phase + (((long long)m * npairs + (valid ? p : 0)) * ncm + pcomp0) * 2;
 #pragma unroll
       for (int j = 0; j < NT; ++j) {
-        const double2 qn = valid ? src[4 * j + 0] : make_double2(0.0, 0.0);
-        const double2 un = valid ? src[4 * j + 2] : make_double2(0.0, 0.0);
-        double2 qs = has_s ? src[4 * j + 1] : make_double2(0.0, 0.0);
-        double2 us = has_s ? src[4 * j + 3] : make_double2(0.0, 0.0);
+        const long long rq = phase_row(valid ? p : 0, ncm, pcomp0 + 2 * j, 0, ms);
+        const long long ru = phase_row(valid ? p : 0, ncm, pcomp0 + 2 * j + 1, 0, ms);
+        const double2 qn = valid ? phase[rq + m] : make_double2(0.0, 0.0);
+        const double2 un = valid ? phase[ru + m] : make_double2(0.0, 0.0);
+        double2 qs = has_s ? phase[rq + ms + m] : make_double2(0.0, 0.0);
+        double2 us = has_s ? phase[ru + ms + m] : make_double2(0.0, 0.0);
         qs.x *= flip; qs.y *= flip; us.x *= flip; us.y *= flip;
         P1q[r][j] = make_double2(qn.x + qs.x, qn.y + qs.y);
         P2q[r][j] = make_double2(qn.x - qs.x, qn.y - qs.y);
@@ -614,81 +711,74 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       }
     }
 
-    for (int lb = mhi; lb <= lmax; lb += LB) {
-      double v[32];
+    for (int ch = 0; ch < nchunks; ++ch) {
+      __pipeline_wait_prior(1);
+      __syncthreads();
+      stage(ch + 2);
+      const double2 *cab = s_ab[ch % 3];
+#pragma unroll 1
+      for (int sb = 0; sb < kChunk; sb += LB) {
+        double v[32];
 #pragma unroll
-      for (int k = 0; k < 32; ++k) v[k] = 0.0;
-      bool any = false;
+        for (int k = 0; k < 32; ++k) v[k] = 0.0;
 #pragma unroll
-      for (int i = 0; i < LB; i += 2) {
-        const int l = lb + i;
-        const double a0 = __ldg(aa + l), b0 = __ldg(bb + l);
-        const double a1 = __ldg(aa + l + 1), b1 = __ldg(bb + l + 1);
+        for (int i = 0; i < LB; i += 2) {
+          const double2 ab0 = cab[sb + i], ab1 = cab[sb + i + 1];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (act[r]) {  // even offset: px = p1, py = p2
+              const double lw = mp1[r] + mm1[r], lx = mm1[r] - mp1[r];
+#pragma unroll
+              for (int j = 0; j < NT; ++j) {
+                const int o = i * VPL + 4 * j;
+                v[o + 0] = fma(lw, P1q[r][j].x, fma(-lx, P2u[r][j].y, v[o + 0]));
+                v[o + 1] = fma(lw, P1q[r][j].y, fma(lx, P2u[r][j].x, v[o + 1]));
+                v[o + 2] = fma(lw, P1u[r][j].x, fma(lx, P2q[r][j].y, v[o + 2]));
+                v[o + 3] = fma(lw, P1u[r][j].y, fma(-lx, P2q[r][j].x, v[o + 3]));
+              }
+            }
+            const double np_ = fma(fma(ab0.x, x[r], -ab0.y), mp1[r], -mp0[r]);
+            const double nm_ = fma(fma(ab0.x, x[r], ab0.y), mm1[r], -mm0[r]);
+            if (act[r]) {  // odd offset: px = p2, py = p1
+              const double lw = np_ + nm_, lx = nm_ - np_;
+#pragma unroll
+              for (int j = 0; j < NT; ++j) {
+                const int o = (i + 1) * VPL + 4 * j;
+                v[o + 0] = fma(lw, P2q[r][j].x, fma(-lx, P1u[r][j].y, v[o + 0]));
+                v[o + 1] = fma(lw, P2q[r][j].y, fma(lx, P1u[r][j].x, v[o + 1]));
+                v[o + 2] = fma(lw, P2u[r][j].x, fma(lx, P1q[r][j].y, v[o + 2]));
+                v[o + 3] = fma(lw, P2u[r][j].y, fma(-lx, P1q[r][j].x, v[o + 3]));
+              }
+            }
+            const double nnp = fma(fma(ab1.x, x[r], -ab1.y), np_, -mp1[r]);
+            const double nnm = fma(fma(ab1.x, x[r], ab1.y), nm_, -mm1[r]);
+            mp0[r] = np_;
+            mp1[r] = nnp;
+            mm0[r] = nm_;
+            mm1[r] = nnm;
+          }
+        }
+        bool any = false;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          if (act[r]) {  // even offset: px = p1, py = p2
-            const double lw = mp1[r] + mm1[r], lx = mm1[r] - mp1[r];
-#pragma unroll
-            for (int j = 0; j < NT; ++j) {
-              double *o = v + i * VPL + 4 * j;
-              o[0] = fma(lw, P1q[r][j].x, fma(-lx, P2u[r][j].y, o[0]));
-              o[1] = fma(lw, P1q[r][j].y, fma(lx, P2u[r][j].x, o[1]));
-              o[2] = fma(lw, P1u[r][j].x, fma(lx, P2q[r][j].y, o[2]));
-              o[3] = fma(lw, P1u[r][j].y, fma(-lx, P2q[r][j].x, o[3]));
-            }
-          }
-          const double np_ = fma(fma(a0, x[r], -b0), mp1[r], -mp0[r]);
-          const double nm_ = fma(fma(a0, x[r], b0), mm1[r], -mm0[r]);
-          if (act[r]) {  // odd offset: px = p2, py = p1
-            const double lw = np_ + nm_, lx = nm_ - np_;
-#pragma unroll
-            for (int j = 0; j < NT; ++j) {
-              double *o = v + (i + 1) * VPL + 4 * j;
-              o[0] = fma(lw, P2q[r][j].x, fma(-lx, P1u[r][j].y, o[0]));
-              o[1] = fma(lw, P2q[r][j].y, fma(lx, P1u[r][j].x, o[1]));
-              o[2] = fma(lw, P2u[r][j].x, fma(lx, P1q[r][j].y, o[2]));
-              o[3] = fma(lw, P2u[r][j].y, fma(-lx, P1q[r][j].x, o[3]));
-            }
-          }
-          const double nnp = fma(fma(a1, x[r], -b1), np_, -mp1[r]);
-          const double nnm = fma(fma(a1, x[r], b1), nm_, -mm1[r]);
-          mp0[r] = np_;
-          mp1[r] = nnp;
-          mm0[r] = nm_;
-          mm1[r] = nnm;
+          any |= act[r];
+          if (((sb + LB) % kLBlock) == 0)
+            spin_renorm(live[r], act[r], mp0[r], mp1[r], mm0[r], mm1[r], Ep[r], Em[r]);
         }
-      }
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        any |= act[r];
-        if (live[r] && !act[r]) {
-          const bool lp = renorm_pair(mp1[r], mp0[r], Ep[r]);
-          const bool lm = renorm_pair(mm1[r], mm0[r], Em[r]);
-          live[r] = lp || lm;
-          const int emax = max(lp ? Ep[r] : -0x3fffffff, lm ? Em[r] : -0x3fffffff);
-          if (live[r] && emax >= -kSwitchExp) {
-            mp1[r] = ldexp(mp1[r], Ep[r]);
-            mp0[r] = ldexp(mp0[r], Ep[r]);
-            mm1[r] = ldexp(mm1[r], Em[r]);
-            mm0[r] = ldexp(mm0[r], Em[r]);
-            act[r] = true;
-          }
+        any = __any_sync(0xffffffffu, any);
+        red[buf][warp][lane] = any ? warp_transpose_reduce32(v) : 0.0;
+        if (__syncthreads_or(any) && warp == 0) {
+          const double acc = (red[buf][0][lane] + red[buf][1][lane]) +
+                             (red[buf][2][lane] + red[buf][3][lane]);
+          const int l = mhi + ch * kChunk + sb + lane / VPL;
+          const int k = lane % VPL;
+          Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
         }
+        buf ^= 1;
       }
-      if (!__syncthreads_or(any)) continue;
-      const double sacc = warp_transpose_reduce32(v);
-      red[warp][lane] = sacc;
-      __syncthreads();
-      if (warp == 0) {
-        double acc = 0.0;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) acc += red[w][lane];
-        const int l = lb + lane / VPL;
-        const int k = lane % VPL;
-        Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
-      }
-      __syncthreads();
     }
+    __pipeline_wait_prior(0);
+    __syncthreads();
   }
 }
 
@@ -722,7 +812,7 @@ void launch_legendre_synth(const JobDesc &job, const GeomPlan &gp, const CoefPla
 #define SHT_S0(NTV)                                                                           \
   synth_spin0_kernel<NTV, R><<<nitems, 128, 0, st>>>(                                         \
       gp.items, gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.seed, A, ncA, comp0, \
-      job.lmax, gp.npairs, phase, ncm, pcomp0)
+      job.lmax, phase, ncm, pcomp0, job.mmax + 1)
     if (nt == 1) SHT_S0(1);
     else if (nt == 2) SHT_S0(2);
     else SHT_S0(4);
@@ -731,7 +821,7 @@ void launch_legendre_synth(const JobDesc &job, const GeomPlan &gp, const CoefPla
 #define SHT_SS(NTV, DV)                                                                         \
   synth_spin_kernel<NTV, R, DV><<<nitems, 128, 0, st>>>(                                        \
       gp.items, gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.beta, cp.seed,        \
-      cp.seed_exp, cp.spin, A, ncA, comp0, job.lmax, gp.npairs, phase, ncm, pcomp0)
+      cp.seed_exp, cp.spin, A, ncA, comp0, job.lmax, phase, ncm, pcomp0, job.mmax + 1)
     if (deriv) {
       if (nt == 1) SHT_SS(1, true);
       else SHT_SS(2, true);
@@ -751,18 +841,18 @@ void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan
   ProfScope ps("legendre_anal", st);
   if (job.spin == 0) {
 #define SHT_A0(NTV)                                                                       \
-  anal_spin0_kernel<NTV, 2><<<nblocks, 256, 0, st>>>(                                     \
+  anal_spin0_kernel<NTV, 4><<<nblocks, 128, 0, st>>>(                                     \
       gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.seed, phase, ncm, pcomp0, \
-      job.lmax, gp.npairs, Aout, ncA, comp0)
+      job.lmax, job.mmax + 1, Aout, ncA, comp0)
     if (nt == 1) SHT_A0(1);
     else if (nt == 2) SHT_A0(2);
     else SHT_A0(4);
 #undef SHT_A0
   } else {
 #define SHT_AS(NTV)                                                                        \
-  anal_spin_kernel<NTV, 1><<<nblocks, 256, 0, st>>>(                                       \
+  anal_spin_kernel<NTV, 2><<<nblocks, 128, 0, st>>>(                                       \
       gp.count, gp.cth, gp.sth, gp.nph, cp.d_moff, cp.alpha, cp.beta, cp.seed, cp.seed_exp, \
-      cp.spin, phase, ncm, pcomp0, job.lmax, gp.npairs, Aout, ncA, comp0)
+      cp.spin, phase, ncm, pcomp0, job.lmax, job.mmax + 1, Aout, ncA, comp0)
     if (nt == 1) SHT_AS(1);
     else SHT_AS(2);
 #undef SHT_AS

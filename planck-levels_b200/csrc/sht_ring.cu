@@ -41,21 +41,98 @@ __device__ __forceinline__ double2 cscale(double2 a, double s) {
   return make_double2(a.x * s, a.y * s);
 }
 
-// One Stockham pass of radix R: Ns = product of the radices already done.
-// out[(j/Ns)*Ns*R + k + q*Ns] = sum_r in[j + r*N/R] w_N^{sign r (N/(Ns R)) (k + q Ns)}
-__device__ void stockham_pass(const double2 *src, double2 *dst, int N, int R, int Ns, bool inv,
-                              const double2 *__restrict__ W, int step) {
+// ---------------------------------------------------------------------------
+// Stockham auto-sort passes.  For radix R and Ns = product of the radices
+// already applied, butterfly j (0 <= j < N/R, k = j mod Ns) reads
+// x_r = src[j + r N/R], twiddles x_r *= w_N^{+-r k N/(Ns R)}, applies the
+// R-point DFT and writes y_q to dst[(j - k) R + k + q Ns].
+// ---------------------------------------------------------------------------
+constexpr double kC5a = 0.30901699437494742410;   // cos(2 pi/5)
+constexpr double kC5b = -0.80901699437494742410;  // cos(4 pi/5)
+constexpr double kS5a = 0.95105651629515357212;   // sin(2 pi/5)
+constexpr double kS5b = 0.58778525229247312917;   // sin(4 pi/5)
+constexpr double kS3 = 0.86602540378443864676;    // sin(2 pi/3)
+
+__device__ __forceinline__ double2 mul_i(double2 a) { return make_double2(-a.y, a.x); }
+
+template <int R>
+__device__ __forceinline__ void small_dft(double2 (&v)[R], bool inv) {
+  if constexpr (R == 2) {
+    const double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    const double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+    const double2 c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+    const double2 id = mul_i(d);  // i d
+    v[0] = cadd(a, c);
+    v[2] = csub(a, c);
+    v[1] = inv ? cadd(b, id) : csub(b, id);
+    v[3] = inv ? csub(b, id) : cadd(b, id);
+  } else if constexpr (R == 3) {
+    const double2 t = cadd(v[1], v[2]);
+    const double2 u = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
+    const double2 d = cscale(mul_i(csub(v[1], v[2])), inv ? kS3 : -kS3);
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(u, d);
+    v[2] = csub(u, d);
+  } else if constexpr (R == 5) {
+    const double2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    const double2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    const double2 x0 = v[0];
+    const double2 r1 = make_double2(x0.x + kC5a * a1.x + kC5b * a2.x, x0.y + kC5a * a1.y + kC5b * a2.y);
+    const double2 r2 = make_double2(x0.x + kC5b * a1.x + kC5a * a2.x, x0.y + kC5b * a1.y + kC5a * a2.y);
+    const double sg = inv ? 1.0 : -1.0;
+    const double2 i1 = cscale(mul_i(make_double2(kS5a * b1.x + kS5b * b2.x, kS5a * b1.y + kS5b * b2.y)), sg);
+    const double2 i2 = cscale(mul_i(make_double2(kS5b * b1.x - kS5a * b2.x, kS5b * b1.y - kS5a * b2.y)), sg);
+    v[0] = make_double2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+    v[1] = cadd(r1, i1);
+    v[4] = csub(r1, i1);
+    v[2] = cadd(r2, i2);
+    v[3] = csub(r2, i2);
+  }
+}
+
+template <int R>
+__device__ void stockham_small(const double2 *src, double2 *dst, int N, int Ns, bool inv,
+                               const double2 *__restrict__ W, int step) {
+  const int NR = N / R;
+  const int sf = N / (Ns * R);
+  for (int j = threadIdx.x; j < NR; j += blockDim.x) {
+    const int k = j % Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * NR];
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        double2 w = __ldg(W + (long long)r * k * sf * step);
+        if (inv) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    small_dft<R>(v, inv);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst[base + q * Ns] = v[q];
+  }
+}
+
+// Generic prime radix: each thread computes whole outputs (parallel over
+// the N outputs, so a large prime factor does not serialise a few threads).
+__device__ void stockham_generic(const double2 *src, double2 *dst, int N, int R, int Ns,
+                                 bool inv, const double2 *__restrict__ W, int step) {
   const int NR = N / R;
   const int sf = N / (Ns * R);
   for (int item = threadIdx.x; item < N; item += blockDim.x) {
     const int j = item / R;
     const int q = item - j * R;
     const int k = j % Ns;
-    int ang = (sf * (k + q * Ns)) % N;
+    const int ang = (sf * (k + q * Ns)) % N;
     int e = 0;
     double2 acc = make_double2(0.0, 0.0);
     for (int r = 0; r < R; ++r) {
-      double2 w = __ldg(W + e * step);
+      double2 w = __ldg(W + (long long)e * step);
       if (inv) w.y = -w.y;
       const double2 v = src[j + r * NR];
       acc.x = fma(v.x, w.x, fma(-v.y, w.y, acc.x));
@@ -63,12 +140,13 @@ __device__ void stockham_pass(const double2 *src, double2 *dst, int N, int R, in
       e += ang;
       if (e >= N) e -= N;
     }
-    dst[(j / Ns) * Ns * R + k + q * Ns] = acc;
+    dst[(j - k) * R + k + q * Ns] = acc;
   }
 }
 
 // Complex FFT of length d.N in buffers a/b; returns the buffer holding the
-// result.  Callers synchronise before and after.
+// result.  Callers synchronise before; the function synchronises after each
+// pass.
 __device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv,
                             const double2 *__restrict__ twiddle) {
   const double2 *W = twiddle + d.tw;
@@ -77,7 +155,13 @@ __device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv,
   double2 *src = a, *dst = b;
   for (int s = 0; s < d.nrad; ++s) {
     const int R = d.rad[s];
-    stockham_pass(src, dst, d.N, R, Ns, inv, W, step);
+    switch (R) {
+      case 2: stockham_small<2>(src, dst, d.N, Ns, inv, W, step); break;
+      case 3: stockham_small<3>(src, dst, d.N, Ns, inv, W, step); break;
+      case 4: stockham_small<4>(src, dst, d.N, Ns, inv, W, step); break;
+      case 5: stockham_small<5>(src, dst, d.N, Ns, inv, W, step); break;
+      default: stockham_generic(src, dst, d.N, R, Ns, inv, W, step); break;
+    }
     __syncthreads();
     Ns *= R;
     double2 *t = src;
@@ -87,30 +171,155 @@ __device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv,
   return src;
 }
 
+// ---------------------------------------------------------------------------
+// Bluestein transform for lengths with large prime factors:
+// X_k = c_k sum_j (x_j c_j) conj(c_{k-j}), c_j = exp(-pi i j^2/N), evaluated
+// as a power-of-two convolution of length M >= 2N-1: in-place radix-2
+// decimation-in-frequency (bit-reversed output), product with the chirp
+// transform precomputed in the same order, decimation-in-time back to
+// natural order.  The inverse transform is conj(forward(conj x)).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 chirp_of(int j, int n, int N, const double2 *__restrict__ Wn) {
+  if ((n & 1) == 0) return __ldg(Wn + (int)(((long long)j * j) % n));  // exp(-2 pi i (j^2 mod n)/n)
+  double sn, cs;
+  sincospi(-double(((long long)j * j) % (2ll * n)) / n, &sn, &cs);
+  return make_double2(cs, sn);
+}
+
+__device__ void dif_inplace(double2 *a, int M, const double2 *__restrict__ Wp, int P) {
+  int lg = 31 - __clz(M);
+  for (int len = M; len >= 2; len >>= 1, --lg) {
+    const int half = len >> 1, st = P / len;
+    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
+      const int blk = t >> (lg - 1), i = t & (half - 1);
+      const int b0 = blk * len + i;
+      const double2 u = a[b0], v = a[b0 + half];
+      a[b0] = cadd(u, v);
+      a[b0 + half] = cmul(csub(u, v), __ldg(Wp + i * st));
+    }
+    __syncthreads();
+  }
+}
+
+__device__ void dit_inplace_inv(double2 *a, int M, const double2 *__restrict__ Wp, int P) {
+  int lg = 1;
+  for (int len = 2; len <= M; len <<= 1, ++lg) {
+    const int half = len >> 1, st = P / len;
+    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
+      const int blk = t >> (lg - 1), i = t & (half - 1);
+      const int b0 = blk * len + i;
+      const double2 u = a[b0], v = cmul(a[b0 + half], cconj(__ldg(Wp + i * st)));
+      a[b0] = cadd(u, v);
+      a[b0 + half] = csub(u, v);
+    }
+    __syncthreads();
+  }
+}
+
+// Input x in buf[0, N); buf holds M entries.  Result in buf[0, N).
+__device__ void run_bluestein(const FftDesc &d, double2 *buf, bool inv,
+                              const double2 *__restrict__ twiddle,
+                              const double2 *__restrict__ wpow2, int P,
+                              const double2 *__restrict__ bhat) {
+  const double2 *Wn = twiddle + d.tw;
+  const double2 *bh = bhat + d.bhat;
+  for (int j = threadIdx.x; j < d.M; j += blockDim.x) {
+    if (j < d.N) {
+      double2 x = buf[j];
+      if (inv) x.y = -x.y;
+      buf[j] = cmul(x, chirp_of(j, d.n, d.N, Wn));
+    } else {
+      buf[j] = make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  dif_inplace(buf, d.M, wpow2, P);
+  for (int k = threadIdx.x; k < d.M; k += blockDim.x) buf[k] = cmul(buf[k], __ldg(bh + k));
+  __syncthreads();
+  dit_inplace_inv(buf, d.M, wpow2, P);
+  for (int k = threadIdx.x; k < d.N; k += blockDim.x) {
+    double2 y = cmul(buf[k], chirp_of(k, d.n, d.N, Wn));
+    if (inv) y.y = -y.y;
+    buf[k] = y;
+  }
+  __syncthreads();
+}
+
+// Precomputes, per Bluestein length, DIF(b)/M with b_j = conj(c_j) for
+// |j| < N (negative j wrapped to M-j).  One CTA per length, in global memory.
+__global__ void bluestein_setup_kernel(const FftDesc *__restrict__ fdesc,
+                                       const int *__restrict__ blue_idx,
+                                       const double2 *__restrict__ twiddle,
+                                       const double2 *__restrict__ wpow2, int P,
+                                       double2 *__restrict__ bhat) {
+  const FftDesc d = fdesc[blue_idx[blockIdx.x]];
+  double2 *b = bhat + d.bhat;
+  const double2 *Wn = twiddle + d.tw;
+  for (int j = threadIdx.x; j < d.M; j += blockDim.x) {
+    int jj = -1;
+    if (j < d.N) jj = j;
+    else if (j > d.M - d.N) jj = d.M - j;
+    b[j] = (jj >= 0) ? cconj(chirp_of(jj, d.n, d.N, Wn)) : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  dif_inplace(b, d.M, wpow2, P);
+  const double inv_m = 1.0 / d.M;
+  for (int j = threadIdx.x; j < d.M; j += blockDim.x) b[j] = cscale(b[j], inv_m);
+}
+
 template <typename T>
 __device__ __forceinline__ void store_px(T *p, double v, bool add) {
   if (add) *p += T(v);
   else *p = T(v);
 }
 
+// e^{i m phi0} for m <= mm as hi[m >> 6] * lo[m & 63], built per ring in
+// shared memory (about 64 + mm/64 sincos calls instead of mm).
+constexpr int kShiftLo = 64;
+__device__ void build_shift(double2 *lo, double2 *hi, int mm, double ph) {
+  const int nhi = (mm >> 6) + 1;
+  for (int t = threadIdx.x; t < kShiftLo + nhi; t += blockDim.x) {
+    double sn, cs;
+    if (t < kShiftLo) {
+      sincos(t * ph, &sn, &cs);
+      lo[t] = make_double2(cs, sn);
+    } else {
+      sincos(double(t - kShiftLo) * kShiftLo * ph, &sn, &cs);
+      hi[t - kShiftLo] = make_double2(cs, sn);
+    }
+  }
+}
+
+__device__ __forceinline__ double2 shift_of(const double2 *lo, const double2 *hi, int m) {
+  return cmul(hi[m >> 6], lo[m & (kShiftLo - 1)]);
+}
+
 // ---------------------------------------------------------------------------
-// phase -> ring (synthesis)
+// phase -> ring (synthesis).  Grid: (pairs of one size class, components).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256)
-phase2ring_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
-                  const long long *__restrict__ ofs, const int *__restrict__ stride,
-                  const double *__restrict__ phi0, const double *__restrict__ weight,
-                  const int *__restrict__ fftidx, const FftDesc *__restrict__ fdesc,
-                  const double2 *__restrict__ twiddle, const double2 *__restrict__ phase,
-                  int ncm, int npairs, int mmax, int flags, T *const *__restrict__ maps,
-                  long long map_lo) {
+__global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
+                                  const int *__restrict__ nph, const long long *__restrict__ ofs,
+                                  const int *__restrict__ stride, const double *__restrict__ phi0,
+                                  const double *__restrict__ weight, const int *__restrict__ fftidx,
+                                  const FftDesc *__restrict__ fdesc,
+                                  const double2 *__restrict__ twiddle,
+                                  const double2 *__restrict__ wpow2, int P,
+                                  const double2 *__restrict__ bhat,
+                                  const double2 *__restrict__ phase, int ncm, int mmax, int flags,
+                                  int nbufA, int nbufB, T *const *__restrict__ maps,
+                                  long long map_lo) {
   extern __shared__ double2 smem[];
-  const int p = blockIdx.x;
+  const int p = pairs[blockIdx.x];
   const int c = blockIdx.y;
+  const int ms = mmax + 1;
   const int mm = min(mmax, mlim[p]);
   const bool add = (flags & SHARP_ADD) != 0;
-  double wscale = (flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0;
+  const double wscale = (flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0;
+  double2 *bufA = smem;
+  double2 *bufB = smem + nbufA;
+  double2 *slo = smem + nbufA + nbufB;
+  double2 *shi = slo + kShiftLo;
   T *map = maps[c];
   for (int h = 0; h < 2; ++h) {
     const int ring = 2 * p + h;
@@ -121,30 +330,23 @@ phase2ring_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
     const double ph = phi0[ring];
     const bool rot = fabs(ph) >= 1e-14;
     const int half = n / 2;  // highest bin kept (n odd: (n-1)/2)
-    double2 *bufA = smem;
-    double2 *bufB = smem + (d.N + 2);
     double2 *C = bufB;
-    const double2 *src = phase + ((long long)p * ncm + c) * 2 + h;
-    const long long mstride = (long long)npairs * ncm * 2;
-    // fold phase[m] * wgt * e^{i m phi0} into bins 0..half (sharp.c:265-300)
+    const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
+    if (rot) {
+      build_shift(slo, shi, mm, ph);
+      __syncthreads();
+    }
+    // fold phase_m * wgt * e^{i m phi0} into bins 0..half (sharp.c:265-300)
     for (int k = threadIdx.x; k <= half; k += blockDim.x) {
       double2 acc = make_double2(0.0, 0.0);
       for (int m = k; m <= mm; m += n) {
-        double2 t = cscale(src[m * mstride], wgt);
-        if (rot) {
-          double sn, cs;
-          sincos(m * ph, &sn, &cs);
-          t = cmul(t, make_double2(cs, sn));
-        }
+        double2 t = cscale(src[m], wgt);
+        if (rot) t = cmul(t, shift_of(slo, shi, m));
         acc = cadd(acc, t);
       }
       for (int m = (k == 0) ? n : n - k; m <= mm; m += n) {
-        double2 t = cscale(src[m * mstride], wgt);
-        if (rot) {
-          double sn, cs;
-          sincos(m * ph, &sn, &cs);
-          t = cmul(t, make_double2(cs, sn));
-        }
+        double2 t = cscale(src[m], wgt);
+        if (rot) t = cmul(t, shift_of(slo, shi, m));
         acc = cadd(acc, cconj(t));
       }
       if (k == 0 || 2 * k == n) acc.y = 0.0;
@@ -156,17 +358,23 @@ phase2ring_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
       // Z_k = (C_k + conj C_{N-k}) + i conj(W^k) (C_k - conj C_{N-k}), k < N
       for (int k = threadIdx.x; k < d.N; k += blockDim.x) {
         const double2 ck = C[k], cn = cconj(C[d.N - k]);
-        const double2 s = cadd(ck, cn), df = csub(ck, cn);
-        const double2 w = __ldg(W + k);  // exp(-2 pi i k/n)
+        const double2 sm = cadd(ck, cn), df = csub(ck, cn);
+        const double2 w = __ldg(W + k);             // exp(-2 pi i k/n)
         const double2 iw = make_double2(w.y, w.x);  // i * conj(w)
-        bufA[k] = cadd(s, cmul(iw, df));
+        bufA[k] = cadd(sm, cmul(iw, df));
       }
     } else {
       for (int k = threadIdx.x; k < n; k += blockDim.x)
         bufA[k] = (k <= half) ? C[k] : cconj(C[n - k]);
     }
     __syncthreads();
-    double2 *res = run_fft(d, bufA, bufB, true, twiddle);
+    double2 *res;
+    if (d.blue) {
+      run_bluestein(d, bufA, true, twiddle, wpow2, P, bhat);
+      res = bufA;
+    } else {
+      res = run_fft(d, bufA, bufB, true, twiddle);
+    }
     const long long o = ofs[ring] - map_lo;
     const long long st = stride[ring];
     if ((n & 1) == 0) {
@@ -186,19 +394,26 @@ phase2ring_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
 // ring -> phase (analysis)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256)
-ring2phase_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
-                  const long long *__restrict__ ofs, const int *__restrict__ stride,
-                  const double *__restrict__ phi0, const double *__restrict__ weight,
-                  const int *__restrict__ fftidx, const FftDesc *__restrict__ fdesc,
-                  const double2 *__restrict__ twiddle, double2 *__restrict__ phase, int ncm,
-                  int npairs, int mmax, int flags, const T *const *__restrict__ maps,
-                  long long map_lo) {
+__global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
+                                  const int *__restrict__ nph, const long long *__restrict__ ofs,
+                                  const int *__restrict__ stride, const double *__restrict__ phi0,
+                                  const double *__restrict__ weight, const int *__restrict__ fftidx,
+                                  const FftDesc *__restrict__ fdesc,
+                                  const double2 *__restrict__ twiddle,
+                                  const double2 *__restrict__ wpow2, int P,
+                                  const double2 *__restrict__ bhat, double2 *__restrict__ phase,
+                                  int ncm, int mmax, int flags, int nbufA, int nbufB,
+                                  const T *const *__restrict__ maps, long long map_lo) {
   extern __shared__ double2 smem[];
-  const int p = blockIdx.x;
+  const int p = pairs[blockIdx.x];
   const int c = blockIdx.y;
+  const int ms = mmax + 1;
   const int mm = min(mmax, mlim[p]);
   const double wscale = (flags & SHARP_REAL_HARMONICS) ? kSqrtTwo : 1.0;
+  double2 *bufA = smem;
+  double2 *bufB = smem + nbufA;
+  double2 *slo = smem + nbufA + nbufB;
+  double2 *shi = slo + kShiftLo;
   const T *map = maps[c];
   for (int h = 0; h < 2; ++h) {
     const int ring = 2 * p + h;
@@ -208,10 +423,9 @@ ring2phase_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
     const double wgt = ((flags & SHARP_USE_WEIGHTS) ? weight[ring] : 1.0) * wscale;
     const double ph = phi0[ring];
     const bool rot = fabs(ph) >= 1e-14;
-    double2 *bufA = smem;
-    double2 *bufB = smem + (d.N + 2);
     const long long o = ofs[ring] - map_lo;
     const long long st = stride[ring];
+    if (rot) build_shift(slo, shi, mm, -ph);
     if ((n & 1) == 0) {
       for (int j = threadIdx.x; j < d.N; j += blockDim.x)
         bufA[j] = make_double2(double(map[o + (2 * j) * st]), double(map[o + (2 * j + 1) * st]));
@@ -220,7 +434,13 @@ ring2phase_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
         bufA[j] = make_double2(double(map[o + j * st]), 0.0);
     }
     __syncthreads();
-    double2 *res = run_fft(d, bufA, bufB, false, twiddle);
+    double2 *res;
+    if (d.blue) {
+      run_bluestein(d, bufA, false, twiddle, wpow2, P, bhat);
+      res = bufA;
+    } else {
+      res = run_fft(d, bufA, bufB, false, twiddle);
+    }
     double2 *X = (res == bufA) ? bufB : bufA;
     const double2 *W = twiddle + d.tw;
     if ((n & 1) == 0) {
@@ -228,10 +448,10 @@ ring2phase_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
       for (int k = threadIdx.x; k <= d.N; k += blockDim.x) {
         const double2 zk = res[k == d.N ? 0 : k];
         const double2 zn = cconj(res[k == 0 ? 0 : d.N - k]);
-        const double2 s = cadd(zk, zn), df = csub(zk, zn);
+        const double2 sm = cadd(zk, zn), df = csub(zk, zn);
         const double2 w = __ldg(W + k);
         const double2 mi_w = make_double2(w.y, -w.x);  // -i * w
-        double2 xk = cscale(cadd(s, cmul(mi_w, df)), 0.5);
+        double2 xk = cscale(cadd(sm, cmul(mi_w, df)), 0.5);
         if (k == 0 || k == d.N) xk.y = 0.0;  // DC and Nyquist are real
         X[k] = xk;
       }
@@ -243,20 +463,13 @@ ring2phase_kernel(const int *__restrict__ mlim, const int *__restrict__ nph,
       }
     }
     __syncthreads();
-    double2 *dst = phase + ((long long)p * ncm + c) * 2 + h;
-    const long long mstride = (long long)npairs * ncm * 2;
+    double2 *dst = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
     for (int m = threadIdx.x; m <= mm; m += blockDim.x) {
       const int idx = m % n;
-      double2 v;
-      if (idx < n - idx) v = X[idx];
-      else v = cconj(X[n - idx]);
+      double2 v = (idx < n - idx) ? X[idx] : cconj(X[n - idx]);
       v = cscale(v, wgt);
-      if (rot) {
-        double sn, cs;
-        sincos(m * ph, &sn, &cs);
-        v = cmul(v, make_double2(cs, -sn));
-      }
-      dst[m * mstride] = v;
+      if (rot) v = cmul(v, shift_of(slo, shi, m));
+      dst[m] = v;
     }
     __syncthreads();
   }
@@ -271,7 +484,7 @@ __global__ void phase2ring_direct_kernel(const int *__restrict__ mlim, const int
                                          const long long *__restrict__ ofs,
                                          const int *__restrict__ stride,
                                          const double *__restrict__ weight,
-                                         const double2 *__restrict__ phase, int ncm, int npairs,
+                                         const double2 *__restrict__ phase, int ncm,
                                          int mmax, int flags, T2 *const *__restrict__ maps,
                                          long long map_lo) {
   const int p = blockIdx.x, c = blockIdx.y;
@@ -284,10 +497,9 @@ __global__ void phase2ring_direct_kernel(const int *__restrict__ mlim, const int
     if (n <= 0) continue;
     double wgt = (flags & SHARP_USE_WEIGHTS) ? n * weight[ring] : 1.0;
     if (flags & SHARP_REAL_HARMONICS) wgt *= kSqrtHalf;
-    const double2 *src = phase + ((long long)p * ncm + c) * 2 + h;
-    const long long mstride = (long long)npairs * ncm * 2;
+    const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * (mmax + 1);
     for (int m = threadIdx.x; m <= mmax; m += blockDim.x) {
-      const double2 v = (m <= mm) ? cscale(src[m * mstride], wgt) : make_double2(0.0, 0.0);
+      const double2 v = (m <= mm) ? cscale(src[m], wgt) : make_double2(0.0, 0.0);
       T2 *px = map + (ofs[ring] - map_lo) + (long long)m * stride[ring];
       if (add) {
         px->x += decltype(px->x)(v.x);
@@ -305,7 +517,7 @@ __global__ void ring2phase_direct_kernel(const int *__restrict__ mlim, const int
                                          const long long *__restrict__ ofs,
                                          const int *__restrict__ stride,
                                          const double *__restrict__ weight,
-                                         double2 *__restrict__ phase, int ncm, int npairs,
+                                         double2 *__restrict__ phase, int ncm,
                                          int mmax, int flags, const T2 *const *__restrict__ maps,
                                          long long map_lo) {
   const int p = blockIdx.x, c = blockIdx.y;
@@ -317,11 +529,10 @@ __global__ void ring2phase_direct_kernel(const int *__restrict__ mlim, const int
     if (n <= 0) continue;
     double wgt = (flags & SHARP_USE_WEIGHTS) ? n * weight[ring] : 1.0;
     if (flags & SHARP_REAL_HARMONICS) wgt *= kSqrtTwo;
-    double2 *dst = phase + ((long long)p * ncm + c) * 2 + h;
-    const long long mstride = (long long)npairs * ncm * 2;
+    double2 *dst = phase + ((long long)(p * ncm + c) * 2 + h) * (mmax + 1);
     for (int m = threadIdx.x; m <= mm; m += blockDim.x) {
       const T2 v = map[(ofs[ring] - map_lo) + (long long)m * stride[ring]];
-      dst[m * mstride] = make_double2(double(v.x) * wgt, double(v.y) * wgt);
+      dst[m] = make_double2(double(v.x) * wgt, double(v.y) * wgt);
     }
   }
 }
@@ -452,52 +663,97 @@ void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
   SHT_CUDA(cudaFreeAsync(d_off, st));
 }
 
-static size_t fft_smem(const GeomPlan &gp) { return sizeof(double2) * 2 * (gp.nmax_complex + 2); }
+// Ring pairs are launched per size class (largest complex FFT length of
+// the pair <= cls_N[c]) so small polar rings do not reserve the shared
+// memory and threads of the largest rings.
+void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cudaStream_t st) {
+  std::vector<int> idx;
+  for (int i = 0; i < int(descs.size()); ++i)
+    if (descs[i].blue) idx.push_back(i);
+  // exp(-2 pi i j/P) for the power-of-two passes (computed even when unused)
+  std::vector<int> pn{gp.P}, po{0};
+  {
+    int *d_n = nullptr, *d_off = nullptr;
+    SHT_CUDA(cudaMallocAsync(&d_n, sizeof(int), st));
+    SHT_CUDA(cudaMallocAsync(&d_off, sizeof(int), st));
+    SHT_CUDA(cudaMemcpyAsync(d_n, pn.data(), sizeof(int), cudaMemcpyHostToDevice, st));
+    SHT_CUDA(cudaMemcpyAsync(d_off, po.data(), sizeof(int), cudaMemcpyHostToDevice, st));
+    ProfScope ps("twiddles", st);
+    twiddle_kernel<<<dim3(8, 1), 256, 0, st>>>(1, d_n, d_off, gp.wpow2);
+    SHT_CUDA(cudaGetLastError());
+    SHT_CUDA(cudaFreeAsync(d_n, st));
+    SHT_CUDA(cudaFreeAsync(d_off, st));
+  }
+  if (idx.empty()) return;
+  int *d_idx = nullptr;
+  SHT_CUDA(cudaMallocAsync(&d_idx, sizeof(int) * idx.size(), st));
+  SHT_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st));
+  ProfScope ps("bluestein_setup", st);
+  bluestein_setup_kernel<<<int(idx.size()), 256, 0, st>>>(gp.fdesc, d_idx, gp.twiddle, gp.wpow2,
+                                                          gp.P, gp.bhat);
+  SHT_CUDA(cudaGetLastError());
+  SHT_CUDA(cudaFreeAsync(d_idx, st));
+}
+
+static size_t fft_smem(const GeomPlan &gp, int cls, int mmax) {
+  return sizeof(double2) * (gp.cls_bufA[cls] + gp.cls_bufB[cls] + 64 + mmax / 64 + 2);
+}
+static int fft_threads(int N) { return N <= 256 ? 64 : N <= 1024 ? 256 : 1024; }
 
 void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                        const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
                        cudaStream_t st) {
-  if (gp.npairs == 0) return;
-  dim3 grid(gp.npairs, nmapptr);
-  const size_t sm = fft_smem(gp);
   ProfScope ps("ring_synth", st);
-  if (job.dp) {
-    auto k = phase2ring_kernel<double>;
-    SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
-                             gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<double *const *>(maps_dev), map_lo);
-  } else {
-    auto k = phase2ring_kernel<float>;
-    SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
-                             gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<float *const *>(maps_dev), map_lo);
+  for (int cls = 0; cls < int(gp.cls_N.size()); ++cls) {
+    if (gp.cls_count[cls] == 0) continue;
+    dim3 grid(gp.cls_count[cls], nmapptr);
+    const size_t sm = fft_smem(gp, cls, job.mmax);
+    const int nbufA = gp.cls_bufA[cls], nbufB = gp.cls_bufB[cls];
+    const int thr = fft_threads(gp.cls_N[cls]);
+    const int *pairs = gp.cls_pairs + gp.cls_start[cls];
+    if (job.dp) {
+      auto k = phase2ring_kernel<double>;
+      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
+                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
+                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<double *const *>(maps_dev), map_lo);
+    } else {
+      auto k = phase2ring_kernel<float>;
+      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
+                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
+                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<float *const *>(maps_dev), map_lo);
+    }
+    SHT_CUDA(cudaGetLastError());
   }
-  SHT_CUDA(cudaGetLastError());
 }
 
 void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                        const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
                        cudaStream_t st) {
-  if (gp.npairs == 0) return;
-  dim3 grid(gp.npairs, nmapptr);
-  const size_t sm = fft_smem(gp);
   ProfScope ps("ring_anal", st);
-  if (job.dp) {
-    auto k = ring2phase_kernel<double>;
-    SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
-                             gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<const double *const *>(maps_dev), map_lo);
-  } else {
-    auto k = ring2phase_kernel<float>;
-    SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    k<<<grid, 256, sm, st>>>(gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight, gp.fft,
-                             gp.fdesc, gp.twiddle, phase, ncm, gp.npairs, job.mmax, job.flags,
-                             reinterpret_cast<const float *const *>(maps_dev), map_lo);
+  for (int cls = 0; cls < int(gp.cls_N.size()); ++cls) {
+    if (gp.cls_count[cls] == 0) continue;
+    dim3 grid(gp.cls_count[cls], nmapptr);
+    const size_t sm = fft_smem(gp, cls, job.mmax);
+    const int nbufA = gp.cls_bufA[cls], nbufB = gp.cls_bufB[cls];
+    const int thr = fft_threads(gp.cls_N[cls]);
+    const int *pairs = gp.cls_pairs + gp.cls_start[cls];
+    if (job.dp) {
+      auto k = ring2phase_kernel<double>;
+      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
+                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
+                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<const double *const *>(maps_dev), map_lo);
+    } else {
+      auto k = ring2phase_kernel<float>;
+      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
+                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
+                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<const float *const *>(maps_dev), map_lo);
+    }
+    SHT_CUDA(cudaGetLastError());
   }
-  SHT_CUDA(cudaGetLastError());
 }
 
 void launch_phase2ring_direct(const JobDesc &job, const GeomPlan &gp, long long map_lo,
@@ -508,11 +764,11 @@ void launch_phase2ring_direct(const JobDesc &job, const GeomPlan &gp, long long 
   ProfScope ps("ring_synth", st);
   if (job.dp)
     phase2ring_direct_kernel<double2><<<grid, 128, 0, st>>>(
-        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
+        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, job.mmax,
         job.flags, reinterpret_cast<double2 *const *>(maps_dev), map_lo);
   else
     phase2ring_direct_kernel<float2><<<grid, 128, 0, st>>>(
-        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
+        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, job.mmax,
         job.flags, reinterpret_cast<float2 *const *>(maps_dev), map_lo);
   SHT_CUDA(cudaGetLastError());
 }
@@ -525,11 +781,11 @@ void launch_ring2phase_direct(const JobDesc &job, const GeomPlan &gp, long long 
   ProfScope ps("ring_anal", st);
   if (job.dp)
     ring2phase_direct_kernel<double2><<<grid, 128, 0, st>>>(
-        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
+        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, job.mmax,
         job.flags, reinterpret_cast<const double2 *const *>(maps_dev), map_lo);
   else
     ring2phase_direct_kernel<float2><<<grid, 128, 0, st>>>(
-        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, gp.npairs, job.mmax,
+        gp.mlim, gp.nph, gp.ofs, gp.stride, gp.weight, phase, ncm, job.mmax,
         job.flags, reinterpret_cast<const float2 *const *>(maps_dev), map_lo);
   SHT_CUDA(cudaGetLastError());
 }
