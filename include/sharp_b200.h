@@ -65,6 +65,25 @@ void sharp_b200_profile (int on);
    *launches (if non-NULL) receives their number. */
 double sharp_b200_profile_ms (const char *family, unsigned long long *launches);
 
+/* Spin-0 alm2map without any device allocation.  No counterpart in the
+   reference: it serves callers that cannot call cudaMalloc when they need a
+   transform (GPU memory owned by another allocator such as a framework's
+   caching pool or an arena reserved at start-up, or a no-allocation policy
+   after initialisation).  Same result as sharp_b200_execute_device(
+   SHARP_ALM2MAP, 0, ..., SHARP_DP) with one transform: alm (complex double,
+   layout alm_info, not SHARP_PACKED) and map (double) are device pointers,
+   ring pixels of map are overwritten, work is enqueued on `stream`.
+   All scratch lives in one fixed 32 MiB __device__ array that every GPU
+   loading the library holds until exit (about Nside 256 / lmax 512 fits);
+   larger problems are rejected: the call returns -1 and
+   sharp_b200_last_error() says how much scratch they would need.  Other
+   failures follow the library's abort policy (in non-abort mode: -1).
+   Returns 0 on success.  The first call on each device looks up the array's
+   address (make it before any stream capture).  All calls share the array:
+   calls that overlap on the GPU race and must be serialised by the caller. */
+int sharp_b200_alm2map_noalloc (const sharp_geom_info *geom_info,
+  const sharp_alm_info *alm_info, const void *alm, void *map, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -126,6 +126,10 @@ void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan
 void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
                      const std::vector<int> &tw_off, cudaStream_t st);
 void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cudaStream_t st);
+void launch_twiddles_preplaced(double2 *tw, const int *d_n, const int *d_off, int ntab,
+                               cudaStream_t st);
+void launch_bluestein_setup_preplaced(const GeomPlan &gp, const int *d_blue_idx, int nblue,
+                                      cudaStream_t st);
 // map_lo / alm_lo: index (in elements of the user array) that the device
 // pointers in maps_dev / alm_dev point at (0 when they are the user's own
 // device arrays, the extent start when they are staged copies).

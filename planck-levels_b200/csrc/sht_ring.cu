@@ -827,4 +827,24 @@ void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
   SHT_CUDA(cudaGetLastError());
 }
 
+// Table set-up without temporary allocations: the caller has already placed
+// the per-table lengths/offsets (and the Bluestein descriptor indices) in
+// device memory.
+void launch_twiddles_preplaced(double2 *tw, const int *d_n, const int *d_off, int ntab,
+                               cudaStream_t st) {
+  if (ntab <= 0) return;
+  ProfScope ps("twiddles", st);
+  twiddle_kernel<<<dim3(8, ntab), 256, 0, st>>>(ntab, d_n, d_off, tw);
+  SHT_CUDA(cudaGetLastError());
+}
+
+void launch_bluestein_setup_preplaced(const GeomPlan &gp, const int *d_blue_idx, int nblue,
+                                      cudaStream_t st) {
+  if (nblue <= 0) return;
+  ProfScope ps("bluestein_setup", st);
+  bluestein_setup_kernel<<<nblue, 256, 0, st>>>(gp.fdesc, d_blue_idx, gp.twiddle, gp.wpow2,
+                                                gp.P, gp.bhat);
+  SHT_CUDA(cudaGetLastError());
+}
+
 }  // namespace sht
