@@ -171,13 +171,14 @@ __device__ __forceinline__ long long phase_row(int p, int ncm, int comp, int h, 
 
 // ---------------------------------------------------------------------------
 // Coefficient staging.  Recurrence coefficients and staged a_lm are consumed
-// in chunks of kChunk l-steps.  Each chunk is copied global -> shared with
-// cp.async into one of three buffers two chunks ahead of its use, so one
-// barrier per chunk both publishes the chunk and frees the buffer the next
-// copy overwrites.  Inside a chunk all lanes read the same shared-memory
-// words (broadcast).
+// in chunks of kChunk l-steps, copied global -> shared with cp.async into one
+// of three buffers two chunks ahead of their use.  Synthesis warps stage
+// privately (a __syncwarp publishes a chunk, no CTA barrier); analysis CTAs
+// share the buffers and merge the publishing barrier with the one of their
+// cross-warp reduction.  Inside a chunk all lanes read the same words.
 // ---------------------------------------------------------------------------
 constexpr int kChunk = 32;
+constexpr int kWarps = 4;  // 128-thread CTAs
 
 __device__ __forceinline__ void copy8(double *dst, const double *src) {
   __pipeline_memcpy_async(dst, src, sizeof(double));
@@ -198,11 +199,12 @@ synth_spin0_kernel(const int2 *__restrict__ items, const int *__restrict__ count
                    const double *__restrict__ alpha, const double *__restrict__ mfac,
                    const double2 *__restrict__ A, int ncA, int comp0, int lmax,
                    double2 *__restrict__ phase, int ncm, int pcomp0, int ms) {
-  __shared__ double s_al[3][kChunk];
-  __shared__ double2 s_A[3][kChunk * NT];
+  __shared__ double s_al[kWarps][3][kChunk];
+  __shared__ double2 s_A[kWarps][3][kChunk * NT];
   const int2 it = items[blockIdx.x];
   const int m = it.x;
   const int cnt = count[m];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long mo = moff[m] - m;  // table index of l is mo + l
   const double *al = alpha + mo;
   const double2 *Am = A + mo * ncA + comp0;
@@ -211,9 +213,9 @@ synth_spin0_kernel(const int2 *__restrict__ items, const int *__restrict__ count
     if (ch < nchunks) {
       const int lc = m + ch * kChunk;
       const int b = ch % 3;
-      for (int t = threadIdx.x; t < kChunk; t += blockDim.x) copy8(&s_al[b][t], al + lc + t);
-      for (int t = threadIdx.x; t < kChunk * NT; t += blockDim.x)
-        copy16(&s_A[b][t], Am + (long long)(lc + t / NT) * ncA + t % NT);
+      for (int t = lane; t < kChunk; t += 32) copy8(&s_al[w][b][t], al + lc + t);
+      for (int t = lane; t < kChunk * NT; t += 32)
+        copy16(&s_A[w][b][t], Am + (long long)(lc + t / NT) * ncA + t % NT);
     }
     __pipeline_commit();
   };
@@ -244,10 +246,10 @@ synth_spin0_kernel(const int2 *__restrict__ items, const int *__restrict__ count
 
   for (int ch = 0; ch < nchunks; ++ch) {
     __pipeline_wait_prior(1);
-    __syncthreads();
+    __syncwarp();
     stage(ch + 2);
-    const double *ca = s_al[ch % 3];
-    const double2 *cA = s_A[ch % 3];
+    const double *ca = s_al[w][ch % 3];
+    const double2 *cA = s_A[w][ch % 3];
 #pragma unroll
     for (int sb = 0; sb < kChunk; sb += kLBlock) {
 #pragma unroll 4
@@ -384,8 +386,9 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
                   double2 *__restrict__ phase, int ncm, int pcomp0, int ms) {
   constexpr int NA = DERIV ? 1 : 2;  // staged alm components per transform
   constexpr int NC = NA * NT;        // staged alm entries per l
-  __shared__ double2 s_ab[3][kChunk];      // (a_l, b_l)
-  __shared__ double2 s_A[3][kChunk * NC];
+  __shared__ double2 s_ab[kWarps][3][kChunk];  // (a_l, b_l)
+  __shared__ double2 s_A[kWarps][3][kChunk * NC];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int2 it = items[blockIdx.x];
   const int m = it.x;
   const int cnt = count[m];
@@ -399,12 +402,12 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
     if (ch < nchunks) {
       const int lc = mhi + ch * kChunk;
       const int b = ch % 3;
-      for (int t = threadIdx.x; t < 2 * kChunk; t += blockDim.x) {
-        double *dst = reinterpret_cast<double *>(&s_ab[b][t >> 1]) + (t & 1);
+      for (int t = lane; t < 2 * kChunk; t += 32) {
+        double *dst = reinterpret_cast<double *>(&s_ab[w][b][t >> 1]) + (t & 1);
         copy8(dst, ((t & 1) ? bb : aa) + lc + (t >> 1));
       }
-      for (int t = threadIdx.x; t < kChunk * NC; t += blockDim.x)
-        copy16(&s_A[b][t], Am + (long long)(lc + t / NC) * ncA + t % NC);
+      for (int t = lane; t < kChunk * NC; t += 32)
+        copy16(&s_A[w][b][t], Am + (long long)(lc + t / NC) * ncA + t % NC);
     }
     __pipeline_commit();
   };
@@ -429,10 +432,10 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
 
   for (int ch = 0; ch < nchunks; ++ch) {
     __pipeline_wait_prior(1);
-    __syncthreads();
+    __syncwarp();
     stage(ch + 2);
-    const double2 *cab = s_ab[ch % 3];
-    const double2 *cA = s_A[ch % 3];
+    const double2 *cab = s_ab[w][ch % 3];
+    const double2 *cA = s_A[w][ch % 3];
 #pragma unroll
     for (int sb = 0; sb < kChunk; sb += kLBlock) {
 #pragma unroll 2
@@ -518,13 +521,27 @@ synth_spin_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
 
 // ---------------------------------------------------------------------------
 // Analysis.  One CTA of 128 threads per m loops over tiles of 128*R ring
-// pairs.  Per l-block every lane accumulates LB*VPL == 32 partial sums over
-// its R rings; a warp transpose-reduction leaves one sum per lane, the four
-// warps are combined in a fixed order and added to Aout (owned by this CTA).
-// Coefficients arrive through the shared-memory chunk pipeline; besides its
-// barrier there is one barrier per l-block (double-buffered reduction
-// scratch).
+// pairs.  Per l-block (LB steps, LB*VPL == 32 values) every lane accumulates
+// its R rings' contributions; a warp transpose-reduction leaves one sum per
+// lane, kept in a per-warp shared array for the whole chunk.  At the next
+// chunk's barrier (the same one that publishes staged coefficients) warp 0
+// adds the four warps' sums in a fixed order to Aout, which this CTA owns:
+// no atomics, bitwise repeatable, one barrier per 32 l-steps.
 // ---------------------------------------------------------------------------
+template <int VPL>
+__device__ __forceinline__ void flush_chunk(const double (*wred)[kChunk * VPL / 32][32], int lane,
+                                            int l0, long long mo, int ncA, int comp0,
+                                            double *__restrict__ Aout) {
+  constexpr int LB = 32 / VPL;
+#pragma unroll 1
+  for (int sb = 0; sb < kChunk / LB; ++sb) {
+    const double acc = (wred[0][sb][lane] + wred[1][sb][lane]) +
+                       (wred[2][sb][lane] + wred[3][sb][lane]);
+    const int l = l0 + sb * LB + lane / VPL;
+    Aout[((mo + l) * ncA + comp0) * 2 + lane % VPL] += acc;
+  }
+}
+
 template <int NT, int R>
 __global__ void __launch_bounds__(128)
 anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
@@ -535,8 +552,9 @@ anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
                   int comp0) {
   constexpr int VPL = 2 * NT;
   constexpr int LB = 32 / VPL;
+  constexpr int NSB = kChunk / LB;
   static_assert(LB % 2 == 0 && kChunk % LB == 0, "l-block must be even and divide a chunk");
-  __shared__ double red[2][4][32];
+  __shared__ double wred[2][kWarps][NSB][32];
   __shared__ double s_al[3][kChunk];
   const int m = blockIdx.x;
   const int cnt = count[m];
@@ -551,7 +569,6 @@ anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         copy8(&s_al[ch % 3][t], al + m + ch * kChunk + t);
     __pipeline_commit();
   };
-  int buf = 0;
 
   for (int tb = 0; tb < cnt; tb += 128 * R) {
     stage(0);
@@ -588,15 +605,18 @@ anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       __pipeline_wait_prior(1);
       __syncthreads();
       stage(ch + 2);
+      if (ch > 0 && warp == 0)
+        flush_chunk<VPL>(wred[(ch - 1) & 1], lane, m + (ch - 1) * kChunk, mo, ncA, comp0, Aout);
       const double *ca = s_al[ch % 3];
 #pragma unroll 1
-      for (int sb = 0; sb < kChunk; sb += LB) {
+      for (int sb = 0; sb < NSB; ++sb) {
         double v[32];
 #pragma unroll
         for (int k = 0; k < 32; ++k) v[k] = 0.0;
+        bool any = false;
 #pragma unroll
         for (int i = 0; i < LB; i += 2) {
-          const double a0 = ca[sb + i], a1 = ca[sb + i + 1];
+          const double a0 = ca[sb * LB + i], a1 = ca[sb * LB + i + 1];
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const double nm = fma(a0 * x[r], mu1[r], -mu0[r]);
@@ -615,11 +635,10 @@ anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
             mu1[r] = nn;
           }
         }
-        bool any = false;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           any |= act[r];
-          if (live[r] && !act[r] && ((sb + LB) % kLBlock) == 0) {
+          if (live[r] && !act[r] && ((sb + 1) * LB) % kLBlock == 0) {
             live[r] = renorm_pair(mu1[r], mu0[r], E[r]);
             if (live[r] && E[r] >= -kSwitchExp) {
               mu1[r] = ldexp(mu1[r], E[r]);
@@ -628,25 +647,25 @@ anal_spin0_kernel(const int *__restrict__ count, const double *__restrict__ cth,
             }
           }
         }
-        any = __any_sync(0xffffffffu, any);
-        red[buf][warp][lane] = any ? warp_transpose_reduce32(v) : 0.0;
-        if (__syncthreads_or(any) && warp == 0) {
-          const double acc = (red[buf][0][lane] + red[buf][1][lane]) +
-                             (red[buf][2][lane] + red[buf][3][lane]);
-          const int l = m + ch * kChunk + sb + lane / VPL;
-          const int k = lane % VPL;
-          Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
-        }
-        buf ^= 1;
+        wred[ch & 1][warp][sb][lane] =
+            __any_sync(0xffffffffu, any) ? warp_transpose_reduce32(v) : 0.0;
       }
     }
     __pipeline_wait_prior(0);
+    __syncthreads();
+    if (warp == 0)
+      flush_chunk<VPL>(wred[(nchunks - 1) & 1], lane, m + (nchunks - 1) * kChunk, mo, ncA, comp0,
+                       Aout);
     __syncthreads();
   }
 }
 
 // Spin-s analysis (E/B from Q/U): per l, (G.re, G.im, C.re, C.im) per
-// transform.  saddstep2, libsharp/sharp_core_inc2.c:338-364.
+// transform (saddstep2, libsharp/sharp_core_inc2.c:338-364), written directly
+// in terms of mu+ and mu- (lw = mu+ + mu-, lx = mu- - mu+):
+//   lw X - lx Y = mu+ (X+Y) + mu- (X-Y),   lw X + lx Y = mu+ (X-Y) + mu- (X+Y)
+// so each output takes 2 FMAs and lw, lx are never formed.  H?p / H?m hold
+// the combined phase factors of mu+ / mu- for even (e) and odd (o) l-mhi.
 template <int NT, int R>
 __global__ void __launch_bounds__(128)
 anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
@@ -658,8 +677,9 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
                  int comp0) {
   constexpr int VPL = 4 * NT;
   constexpr int LB = 32 / VPL;
+  constexpr int NSB = kChunk / LB;
   static_assert(LB % 2 == 0 && kChunk % LB == 0, "l-block must be even and divide a chunk");
-  __shared__ double red[2][4][32];
+  __shared__ double wred[2][kWarps][NSB][32];
   __shared__ double2 s_ab[3][kChunk];
   const int m = blockIdx.x;
   const int cnt = count[m];
@@ -678,7 +698,6 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       }
     __pipeline_commit();
   };
-  int buf = 0;
 
   for (int tb = 0; tb < cnt; tb += 128 * R) {
     stage(0);
@@ -686,7 +705,8 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
     double x[R], mp0[R], mp1[R], mm0[R], mm1[R];
     int Ep[R], Em[R];
     bool act[R], live[R];
-    double2 P1q[R][NT], P1u[R][NT], P2q[R][NT], P2u[R][NT];
+    // [r][j][k]: k = G.re, G.im, C.re, C.im
+    double Hep[R][NT][4], Hem[R][NT][4], Hop[R][NT][4], Hom[R][NT][4];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int p = tb + r * 128 + threadIdx.x;
@@ -704,10 +724,22 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         double2 qs = has_s ? phase[rq + ms + m] : make_double2(0.0, 0.0);
         double2 us = has_s ? phase[ru + ms + m] : make_double2(0.0, 0.0);
         qs.x *= flip; qs.y *= flip; us.x *= flip; us.y *= flip;
-        P1q[r][j] = make_double2(qn.x + qs.x, qn.y + qs.y);
-        P2q[r][j] = make_double2(qn.x - qs.x, qn.y - qs.y);
-        P1u[r][j] = make_double2(un.x + us.x, un.y + us.y);
-        P2u[r][j] = make_double2(un.x - us.x, un.y - us.y);
+        const double2 P1q = make_double2(qn.x + qs.x, qn.y + qs.y);
+        const double2 P2q = make_double2(qn.x - qs.x, qn.y - qs.y);
+        const double2 P1u = make_double2(un.x + us.x, un.y + us.y);
+        const double2 P2u = make_double2(un.x - us.x, un.y - us.y);
+        // even offset: px = p1, py = p2
+        //   G.re = lw P1q.re - lx P2u.im   G.im = lw P1q.im + lx P2u.re
+        //   C.re = lw P1u.re + lx P2q.im   C.im = lw P1u.im - lx P2q.re
+        Hep[r][j][0] = P1q.x + P2u.y; Hem[r][j][0] = P1q.x - P2u.y;
+        Hep[r][j][1] = P1q.y - P2u.x; Hem[r][j][1] = P1q.y + P2u.x;
+        Hep[r][j][2] = P1u.x - P2q.y; Hem[r][j][2] = P1u.x + P2q.y;
+        Hep[r][j][3] = P1u.y + P2q.x; Hem[r][j][3] = P1u.y - P2q.x;
+        // odd offset: px = p2, py = p1
+        Hop[r][j][0] = P2q.x + P1u.y; Hom[r][j][0] = P2q.x - P1u.y;
+        Hop[r][j][1] = P2q.y - P1u.x; Hom[r][j][1] = P2q.y + P1u.x;
+        Hop[r][j][2] = P2u.x - P1q.y; Hom[r][j][2] = P2u.x + P1q.y;
+        Hop[r][j][3] = P2u.y + P1q.x; Hom[r][j][3] = P2u.y - P1q.x;
       }
     }
 
@@ -715,40 +747,40 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       __pipeline_wait_prior(1);
       __syncthreads();
       stage(ch + 2);
+      if (ch > 0 && warp == 0)
+        flush_chunk<VPL>(wred[(ch - 1) & 1], lane, mhi + (ch - 1) * kChunk, mo, ncA, comp0,
+                         Aout);
       const double2 *cab = s_ab[ch % 3];
 #pragma unroll 1
-      for (int sb = 0; sb < kChunk; sb += LB) {
+      for (int sb = 0; sb < NSB; ++sb) {
         double v[32];
 #pragma unroll
         for (int k = 0; k < 32; ++k) v[k] = 0.0;
+        bool any = false;
 #pragma unroll
         for (int i = 0; i < LB; i += 2) {
-          const double2 ab0 = cab[sb + i], ab1 = cab[sb + i + 1];
+          const double2 ab0 = cab[sb * LB + i], ab1 = cab[sb * LB + i + 1];
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            if (act[r]) {  // even offset: px = p1, py = p2
-              const double lw = mp1[r] + mm1[r], lx = mm1[r] - mp1[r];
+            if (act[r]) {
 #pragma unroll
-              for (int j = 0; j < NT; ++j) {
-                const int o = i * VPL + 4 * j;
-                v[o + 0] = fma(lw, P1q[r][j].x, fma(-lx, P2u[r][j].y, v[o + 0]));
-                v[o + 1] = fma(lw, P1q[r][j].y, fma(lx, P2u[r][j].x, v[o + 1]));
-                v[o + 2] = fma(lw, P1u[r][j].x, fma(lx, P2q[r][j].y, v[o + 2]));
-                v[o + 3] = fma(lw, P1u[r][j].y, fma(-lx, P2q[r][j].x, v[o + 3]));
-              }
+              for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                  double &o = v[i * VPL + 4 * j + k];
+                  o = fma(mp1[r], Hep[r][j][k], fma(mm1[r], Hem[r][j][k], o));
+                }
             }
             const double np_ = fma(fma(ab0.x, x[r], -ab0.y), mp1[r], -mp0[r]);
             const double nm_ = fma(fma(ab0.x, x[r], ab0.y), mm1[r], -mm0[r]);
-            if (act[r]) {  // odd offset: px = p2, py = p1
-              const double lw = np_ + nm_, lx = nm_ - np_;
+            if (act[r]) {
 #pragma unroll
-              for (int j = 0; j < NT; ++j) {
-                const int o = (i + 1) * VPL + 4 * j;
-                v[o + 0] = fma(lw, P2q[r][j].x, fma(-lx, P1u[r][j].y, v[o + 0]));
-                v[o + 1] = fma(lw, P2q[r][j].y, fma(lx, P1u[r][j].x, v[o + 1]));
-                v[o + 2] = fma(lw, P2u[r][j].x, fma(lx, P1q[r][j].y, v[o + 2]));
-                v[o + 3] = fma(lw, P2u[r][j].y, fma(-lx, P1q[r][j].x, v[o + 3]));
-              }
+              for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                  double &o = v[(i + 1) * VPL + 4 * j + k];
+                  o = fma(np_, Hop[r][j][k], fma(nm_, Hom[r][j][k], o));
+                }
             }
             const double nnp = fma(fma(ab1.x, x[r], -ab1.y), np_, -mp1[r]);
             const double nnm = fma(fma(ab1.x, x[r], ab1.y), nm_, -mm1[r]);
@@ -758,26 +790,21 @@ anal_spin_kernel(const int *__restrict__ count, const double *__restrict__ cth,
             mm1[r] = nnm;
           }
         }
-        bool any = false;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           any |= act[r];
-          if (((sb + LB) % kLBlock) == 0)
+          if (((sb + 1) * LB) % kLBlock == 0)
             spin_renorm(live[r], act[r], mp0[r], mp1[r], mm0[r], mm1[r], Ep[r], Em[r]);
         }
-        any = __any_sync(0xffffffffu, any);
-        red[buf][warp][lane] = any ? warp_transpose_reduce32(v) : 0.0;
-        if (__syncthreads_or(any) && warp == 0) {
-          const double acc = (red[buf][0][lane] + red[buf][1][lane]) +
-                             (red[buf][2][lane] + red[buf][3][lane]);
-          const int l = mhi + ch * kChunk + sb + lane / VPL;
-          const int k = lane % VPL;
-          Aout[((mo + l) * ncA + comp0) * 2 + k] += acc;
-        }
-        buf ^= 1;
+        wred[ch & 1][warp][sb][lane] =
+            __any_sync(0xffffffffu, any) ? warp_transpose_reduce32(v) : 0.0;
       }
     }
     __pipeline_wait_prior(0);
+    __syncthreads();
+    if (warp == 0)
+      flush_chunk<VPL>(wred[(nchunks - 1) & 1], lane, mhi + (nchunks - 1) * kChunk, mo, ncA,
+                       comp0, Aout);
     __syncthreads();
   }
 }
