@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
               "-I", os.path.join(ROOT, "include"), "-I", CSRC] + ARCH
-SOURCES = ["sht_host.cc", "sht_execute.cu", "sht_legendre.cu", "sht_ring.cu", "sht_profile.cu", "sht_noalloc.cu"]
+SOURCES = ["sht_host.cc", "sht_execute.cu", "sht_legendre.cu", "sht_ring.cu", "sht_profile.cu", "sht_noalloc.cu", "sht_mixed.cu"]
 
 
 def nvcc() -> str:
@@ -37,7 +37,7 @@ def _stale(obj: str, deps: list[str]) -> bool:
 
 def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     objs = []
     for src in SOURCES:

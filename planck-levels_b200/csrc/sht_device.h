@@ -45,10 +45,12 @@ struct GeomPlan {
   std::vector<int> order;            // internal index -> reference pair index
   std::vector<int2> synth_items;     // (m, tile) work list for synthesis
   int synth_tile = 0;
+  std::vector<int2> mixed_items;     // (m, tile of 256 pairs) for the tensor-core path
   // device arrays
   double *cth = nullptr, *sth = nullptr;
   int *mlim = nullptr, *count = nullptr;
   int2 *items = nullptr;
+  int2 *mitems = nullptr;
   // per ring (index 2*p + h)
   double *phi0 = nullptr, *weight = nullptr;
   long long *ofs = nullptr;
@@ -112,6 +114,12 @@ struct JobDesc {
   int lmax, mmax;
   bool dp;
 };
+
+// Mixed-precision tensor-core synthesis (sht_mixed.cu)
+bool mixed_synth_supported(const JobDesc &job);
+void launch_mixed_synth(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
+                        const double2 *A, int ncA, double2 *phase, int ncm, int *d_err,
+                        cudaStream_t st);
 
 // Kernel launchers (sht_legendre.cu)
 void launch_coef_tables(CoefPlan &cp, cudaStream_t st);

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -126,6 +127,8 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   gp->synth_tile = 256;
   for (int m = 0; m <= mmax; ++m)
     for (int t = 0; t * gp->synth_tile < gp->count_m[m]; ++t) gp->synth_items.push_back({m, t});
+  for (int m = 0; m <= mmax; ++m)
+    for (int t = 0; t * 256 < gp->count_m[m]; ++t) gp->mixed_items.push_back({m, t});
 
   std::vector<double> cth(np), sth(np), phi0(2 * np), weight(2 * np);
   std::vector<int> ml_sorted(np), nph(2 * np), stride(2 * np), fft(2 * np, 0);
@@ -255,6 +258,7 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   gp->mlim = dev_upload(ml_sorted, st);
   gp->count = dev_upload(gp->count_m, st);
   gp->items = dev_upload(gp->synth_items, st);
+  gp->mitems = dev_upload(gp->mixed_items, st);
   gp->phi0 = dev_upload(phi0, st);
   gp->weight = dev_upload(weight, st);
   gp->ofs = dev_upload(ofs, st);
@@ -404,6 +408,22 @@ AlmPlan *get_alm_plan(const sharp_alm_info *a, int mmax, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // per-device library stream
 // ---------------------------------------------------------------------------
+// Keeps freed workspace in the device's default pool instead of returning it
+// to the driver at every synchronisation (re-mapping gigabytes of workspace
+// per call costs tens of milliseconds).  Once per device.
+void retain_pool_memory() {
+  static std::set<int> done;
+  int dev = 0;
+  SHT_CUDA(cudaGetDevice(&dev));
+  if (done.count(dev)) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done.insert(dev);
+}
+
 cudaStream_t library_stream() {
   static std::map<int, cudaStream_t> streams;
   int dev = 0;
@@ -412,14 +432,41 @@ cudaStream_t library_stream() {
   if (it != streams.end()) return it->second;
   cudaStream_t s;
   SHT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  // keep freed workspace in the pool instead of returning it to the driver
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t thr = ~0ull;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
   streams[dev] = s;
   return s;
+}
+
+// Error word of the tensor-core kernels: pinned, mapped host memory the
+// kernels store a nonzero value into when a bounded wait gives up.  Read
+// without synchronisation: a host-pointer call checks it after its final
+// synchronisation, a device-pointer call finds a failure of an earlier call
+// at its start.
+int *tc_error_word(int **dev_view) {
+  static int *host = nullptr;
+  static std::map<int, int *> views;
+  if (!host) {
+    SHT_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&host), sizeof(int), cudaHostAllocMapped |
+                           cudaHostAllocPortable));
+    *reinterpret_cast<volatile int *>(host) = 0;
+  }
+  int dev = 0;
+  SHT_CUDA(cudaGetDevice(&dev));
+  auto it = views.find(dev);
+  if (it == views.end()) {
+    int *d = nullptr;
+    SHT_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&d), host, 0));
+    it = views.emplace(dev, d).first;
+  }
+  if (dev_view) *dev_view = it->second;
+  return host;
+}
+
+void check_tc_error() {
+  volatile int *w = tc_error_word(nullptr);
+  if (*w) {
+    *w = 0;
+    fail(__FILE__, __LINE__, "a tensor-core transform gave up waiting on the device (SHARP_MIXED)");
+  }
 }
 
 struct DevBuf {
@@ -471,7 +518,9 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
     flags |= SHARP_USE_WEIGHTS;
   }
   SHT_REQUIRE(spin >= 0 && spin <= ainfo->lmax, "bad spin");
-  SHT_REQUIRE(!(flags & SHARP_MIXED), "SHARP_MIXED is only available through the batched entry");
+  SHT_REQUIRE(!(flags & SHARP_MIXED) || (type == SHARP_ALM2MAP && spin == 0) ||
+                  type == SHARP_MAP2ALM || type == SHARP_ALM2MAP,
+              "SHARP_MIXED applies to alm2map and map2alm jobs");
   // all m from 0 to nm-1 exactly once (sharp_get_mmax, sharp.c:238-251)
   const int nm = ainfo->nm;
   {
@@ -505,6 +554,8 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
     }
 
   std::lock_guard<std::mutex> lk(g_cache_mutex);
+  retain_pool_memory();
+  if (flags & SHARP_MIXED) check_tc_error();
   cudaStream_t st = device_ptrs ? user_stream : library_stream();
   GeomPlan *gp = get_geom_plan(ginfo, job.lmax, mmax, spin, st);
   CoefPlan *cp = get_coef_plan(job.lmax, mmax, spin, st);
@@ -585,11 +636,17 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
     launch_stage_alm(job, *ap, alm_lo, *cp, d_norm.as<double>(),
                      reinterpret_cast<void *const *>(d_almptr.p), nalmptr, d_A.as<double2>(), ncA,
                      st);
-    for (int t0 = 0; t0 < ntrans;) {
-      const int nt = group(ntrans - t0, ntmax_synth);
-      launch_legendre_synth(job, *gp, *cp, d_A.as<double2>(), ncA, t0 * job.nalm, nt, phase, ncm,
-                            t0 * job.nmaps, st);
-      t0 += nt;
+    if ((flags & SHARP_MIXED) && mixed_synth_supported(job)) {
+      int *d_err = nullptr;
+      tc_error_word(&d_err);
+      launch_mixed_synth(job, *gp, *cp, d_A.as<double2>(), ncA, phase, ncm, d_err, st);
+    } else {
+      for (int t0 = 0; t0 < ntrans;) {
+        const int nt = group(ntrans - t0, ntmax_synth);
+        launch_legendre_synth(job, *gp, *cp, d_A.as<double2>(), ncA, t0 * job.nalm, nt, phase,
+                              ncm, t0 * job.nmaps, st);
+        t0 += nt;
+      }
     }
     if (no_fft)
       launch_phase2ring_direct(job, *gp, map_lo, phase, ncm,
@@ -624,7 +681,10 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
         SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(alm_in[i]) + esz_alm * alm_lo, dalm[i],
                                  esz_alm * alm_n, cudaMemcpyDeviceToHost, st));
   }
-  if (!device_ptrs) SHT_CUDA(cudaStreamSynchronize(st));
+  if (!device_ptrs) {
+    SHT_CUDA(cudaStreamSynchronize(st));
+    if (flags & SHARP_MIXED) check_tc_error();
+  }
   owned.clear();
 
   if (opcnt) {
@@ -653,6 +713,7 @@ void guarded(const std::function<void()> &fn) {
 
 GeomPlan::~GeomPlan() {
   dev_free(cth); dev_free(sth); dev_free(mlim); dev_free(count); dev_free(items);
+  dev_free(mitems);
   dev_free(phi0); dev_free(weight); dev_free(ofs); dev_free(nph); dev_free(stride);
   dev_free(fft); dev_free(fdesc); dev_free(twiddle); dev_free(cls_pairs);
   dev_free(bhat); dev_free(wpow2);

@@ -1,0 +1,793 @@
+// Mixed-precision batched synthesis on the 5th-generation tensor cores.
+//
+// For NB transforms sharing geometry and lmax, the Legendre step of alm2map
+// is, per order m and tile of 128 ring pairs, the contraction
+//   R[ring, col] = sum_l lambda_l(ring) * a_l[col]
+// split by the parity of l - max(m, s) (north/south symmetry), with
+// col = (transform, component, re/im).  The recurrence for lambda stays FP64
+// (one thread per ring pair, exponent-tracked as in the FP64 kernels).  The
+// contraction runs exactly in integers on tcgen05.mma.kind::i8:
+//
+//  * lambda is bounded analytically, |lambda_lm| <= sqrt((2l+1)/4pi) for
+//    spin 0 and |d^l_{m,+-s}| <= 1 for spin s (so |r+ +- r-| <= 2), so
+//    q_l = round(lambda_l * 2^30 / b_l) fits 31 bits.  One DFMA with the
+//    constant 1.5*2^52 + 2^31 leaves u_l = q_l + 2^31 in the low word of the
+//    result: its four bytes are the unsigned int8 digits of the A operand,
+//    stored as they are (K index = 4*l + byte).
+//  * a_l * b_l is quantised per (m, column) to p_l = round(. * 2^30 / max),
+//    written as four signed int8 digits d_0..d_3.  The B operand is the
+//    Toeplitz expansion B[(l,k), (col,w)] = d_{w-k}, w = 2..6, so one MMA
+//    accumulates the byte products of equal weight 2^(8w) in one int32
+//    column; products of weight below 2^16 are dropped (relative size 2^-30).
+//  * int32 accumulation over all l is exact (|sum| < 2^29 for lmax <= 8192),
+//    so TMEM is read once per tile; the epilogue forms
+//    sum_w D_w 2^(8w) - 2^31 sum_l p_l in FP64 and rescales.
+//
+// Warp roles (288 threads): warps 0-7 each own 32 ring pairs (two row sets
+// of 128, each its own MMA M dimension and TMEM accumulators, sharing the B
+// tiles), run the recurrence and write the A tiles of a 32-l chunk; lane 0
+// of warp 8 streams the per-chunk block (recurrence coefficients,
+// quantisation factors, B tiles) with cp.async.bulk and issues the MMAs.
+// Chunks are pipelined through mbarriers (A tiles double-buffered,
+// coefficient blocks prefetched four deep); every wait is bounded and a
+// timeout is reported through an error word (mapped host memory) after the
+// accumulators are released.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <vector>
+
+#include "sht_device.h"
+#include "sht_recurrence.cuh"
+
+namespace sht {
+
+namespace {
+
+constexpr int kMC = 32;          // l-steps per chunk
+constexpr int kLP = kMC / 2;     // l-steps of one parity per chunk
+constexpr int kKB = 4 * kLP;     // K bytes of one parity tile (64)
+constexpr int kRows = 128;       // ring pairs per row set (MMA M)
+constexpr int kRS = 2;           // row sets per CTA (256 ring pairs, 8 producer warps)
+constexpr int kClasses = 5;      // byte-product weights 2^16 .. 2^48
+constexpr int kSA = 2;           // A-tile stages
+constexpr int kSB = 4;           // coefficient/B-block stages
+constexpr int kThreads = 32 * (4 * kRS + 1);
+constexpr int kWaitLimit = 1 << 22;
+constexpr double kQ = 1073741824.0;                            // 2^30
+constexpr double kMagic = 6755399441055744.0 + 2147483648.0;   // 1.5*2^52 + 2^31
+constexpr int kTileBytes = kRows * kKB;                        // one A tile (8 KiB)
+
+// --------------------------------------------------------------------------
+// PTX helpers (tcgen05 / mbarrier / bulk copy)
+// --------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+               :: "r"(smem_u32(slot)), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;"
+               :: "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t phase) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(done) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t phase) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(done) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+  return done != 0;
+}
+// Bounded wait (a non-blocking test first: a completed phase costs little);
+// false after kWaitLimit unsuccessful tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
+  if (mbar_test(bar, phase)) return true;
+  for (int i = 0; i < kWaitLimit; ++i)
+    if (mbar_try(bar, phase)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :: "r"(smem_u32(bar)) : "memory");
+}
+// D[tmem] (+)= A(smem) * B(smem)^T, kind::i8 (A unsigned, B signed), int32.
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :: "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z),
+         "r"(z), "r"(z)
+      : "memory");
+}
+// 16 consecutive 32-bit columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_wait() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of
+// 8 rows x 16 bytes; LBO = step between K-adjacent core matrices, SBO = step
+// between 8-row groups (sm_100 descriptor version 1 at bit 46).
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
+}
+// Instruction descriptor: D s32, A u8, B s8, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t make_idesc_i8(int n) {
+  return (2u << 4) | (0u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) |
+         (uint32_t(128 >> 4) << 24);
+}
+
+// Byte offset of element (row, kbyte) in a K-major tile whose rows are
+// kKB bytes long.
+__host__ __device__ constexpr int tile_off(int row, int kb) {
+  return ((row >> 3) * (kKB / 16) + (kb >> 4)) * 128 + (row & 7) * 16 + (kb & 15);
+}
+
+// 2^31 + round(v * cq) (the A operand word; |v * cq| <= 2^30 by the bound)
+__device__ __forceinline__ uint32_t quant(double v, double cq) {
+  return static_cast<uint32_t>(__double2loint(fma(v, cq, kMagic)));
+}
+
+// Shared-memory accesses in explicit form (volatile: they stay behind the
+// mbarrier waits that publish the data).
+__device__ __forceinline__ double2 lds_f64x2(uint32_t a) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts_u32x4(uint32_t a, uint32_t x, uint32_t y, uint32_t z,
+                                          uint32_t w) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" :: "r"(a), "r"(x), "r"(y), "r"(z),
+               "r"(w) : "memory");
+}
+
+// 16 l-steps of the spin-0 recurrence for one ring pair: quantised words of
+// the even-offset (ue) and odd-offset (uo) values.  ALL: every lane of the
+// warp is in the IEEE regime (no per-lane masking of the quantisation).
+template <bool ALL>
+__device__ __forceinline__ void steps16_s0(uint32_t cf, double x, bool act, double &mu0,
+                                           double &mu1, uint32_t *ue, uint32_t *uo) {
+  double2 c[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) c[k] = lds_f64x2(cf + 16 * k);  // (alpha_l, cq_l)
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const double q0 = (ALL || act) ? c[2 * j].y : 0.0;
+    const double q1 = (ALL || act) ? c[2 * j + 1].y : 0.0;
+    ue[j] = quant(mu1, q0);
+    const double nm = fma(c[2 * j].x * x, mu1, -mu0);
+    uo[j] = quant(nm, q1);
+    const double nn = fma(c[2 * j + 1].x * x, nm, -mu1);
+    mu0 = nm;
+    mu1 = nn;
+  }
+}
+
+// 8 l-steps of the spin-s recurrences (mu+, mu-): words of r+ + r- (uw)
+// and r- - r+ (ux), even (e) and odd (o) offsets.
+template <bool ALL>
+__device__ __forceinline__ void steps8_sp(uint32_t cf, double x, bool act, double &mp0,
+                                          double &mp1, double &mm0, double &mm1, uint32_t *uwe,
+                                          uint32_t *uxe, uint32_t *uwo, uint32_t *uxo) {
+  double2 ab[8], cq[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    ab[k] = lds_f64x2(cf + 32 * k);       // (a_l, b_l)
+    cq[k] = lds_f64x2(cf + 32 * k + 16);  // (cq_l, 0)
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const double q0 = (ALL || act) ? cq[2 * j].x : 0.0;
+    const double q1 = (ALL || act) ? cq[2 * j + 1].x : 0.0;
+    {
+      const uint32_t up = quant(mp1, q0), um = quant(mm1, q0);
+      uwe[j] = up + um - 0x80000000u;
+      uxe[j] = um - up + 0x80000000u;
+    }
+    const double2 a0 = ab[2 * j], a1 = ab[2 * j + 1];
+    const double np_ = fma(fma(a0.x, x, -a0.y), mp1, -mp0);
+    const double nm_ = fma(fma(a0.x, x, a0.y), mm1, -mm0);
+    {
+      const uint32_t up = quant(np_, q1), um = quant(nm_, q1);
+      uwo[j] = up + um - 0x80000000u;
+      uxo[j] = um - up + 0x80000000u;
+    }
+    const double nnp = fma(fma(a1.x, x, -a1.y), np_, -mp1);
+    const double nnm = fma(fma(a1.x, x, a1.y), nm_, -mm1);
+    mp0 = np_;
+    mp1 = nnp;
+    mm0 = nm_;
+    mm1 = nnm;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Compile-time shape of one kernel instance.
+// --------------------------------------------------------------------------
+template <int T_, int NCOMP_, int NB_>
+struct Shape {
+  static constexpr int T = T_;                 // value types (1: lambda; 2: r+ + r-, r- - r+)
+  static constexpr int NCOMP = NCOMP_;         // a_lm components per transform
+  static constexpr int NB = NB_;               // transforms per launch
+  static constexpr int NCOL = 2 * NCOMP * NB;  // real columns
+  static constexpr int NPR = kClasses * NCOL;  // B rows used
+  static constexpr int NP = (NPR + 15) / 16 * 16;
+  static constexpr int PS = NP <= 256 ? NP : NP / 2;  // MMA N per instruction
+  static constexpr int CE = (T == 1) ? 16 : 32;       // coefficient bytes per l
+  static constexpr int COEF = kMC * CE;
+  static constexpr int BLK = COEF + 2 * NP * kKB;     // per-chunk block
+  static constexpr int ATILES = T * 2;                // A tiles per row set
+  static constexpr int TCOLS = ATILES * NP;           // TMEM columns per row set
+  static constexpr int ALLCOLS = kRS * TCOLS;
+  static constexpr uint32_t NCOLS =
+      ALLCOLS <= 32 ? 32 : ALLCOLS <= 64 ? 64 : ALLCOLS <= 128 ? 128 : ALLCOLS <= 256 ? 256 : 512;
+  static constexpr int SMEM = kSB * BLK + kSA * kRS * ATILES * kTileBytes;
+  static constexpr int MINB = NCOLS <= 256 ? 2 : 1;   // CTAs per SM the TMEM allows
+  static_assert(NP % PS == 0 && PS % 16 == 0 && PS <= 256, "MMA N shape");
+  static_assert(ALLCOLS <= 512, "TMEM capacity");
+  static_assert(BLK % 16 == 0, "bulk copy granularity");
+};
+
+// --------------------------------------------------------------------------
+// Per-call image of the a_lm and coefficients: per (m, chunk) one block
+// [coefficients | B tile even | B tile odd], plus per-m epilogue constants
+// epi[m] = {scale[col], 2^31 * sum_even p[col], 2^31 * sum_odd p[col]}.
+// One CTA per m; warp w handles the columns col = w (mod 8).  The image is
+// zero-filled beforehand (padding rows and l > lmax stay zero).
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+mixed_image_kernel(int lmax, int spin, int ncol, int ncomp, int NP, int CE, int BLK,
+                   const long long *__restrict__ moff, const double *__restrict__ ca,
+                   const double *__restrict__ cb, const double *__restrict__ cfac,
+                   const long long *__restrict__ ioff, const double2 *__restrict__ A, int ncA,
+                   int comp0, unsigned char *__restrict__ img, double *__restrict__ epi) {
+  const int m = blockIdx.x;
+  const int lbase = max(m, spin);
+  if (lbase > lmax) return;
+  const long long mo = moff[m] - m;
+  const int nch = (lmax - lbase + kMC) / kMC;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *base = img + ioff[m];
+  double *ep = epi + (long long)m * 3 * ncol;
+  auto bound = [&](int l) { return spin == 0 ? sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) : 2.0; };
+  auto bval = [&](int l, int col) -> double {
+    const double c = cfac[mo + l];
+    if (c == 0.0) return 0.0;
+    const int j = col / (2 * ncomp), comp = (col >> 1) % ncomp;
+    const double2 a = A[(mo + l) * ncA + comp0 + ncomp * j + comp];
+    return ((col & 1) ? a.y : a.x) / c * bound(l);
+  };
+  // coefficient blocks: (alpha_l, cq_l) or (a_l, b_l, cq_l, 0)
+  for (int e = threadIdx.x; e < nch * kMC; e += blockDim.x) {
+    const int l = lbase + e;
+    double *cf = reinterpret_cast<double *>(base + (long long)(e / kMC) * BLK) +
+                 (e % kMC) * (CE / 8);
+    const double cq = cfac[mo + l] * kQ / bound(l);
+    cf[0] = ca[mo + l];
+    if (spin == 0) {
+      cf[1] = cq;
+    } else {
+      cf[1] = cb[mo + l];
+      cf[2] = cq;
+      cf[3] = 0.0;
+    }
+  }
+  for (int col = warp; col < ncol; col += 8) {
+    double amax = 0.0;
+    for (int l = lbase + lane; l <= lmax; l += 32) amax = fmax(amax, fabs(bval(l, col)));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    const double inv = amax > 0.0 ? kQ / amax : 0.0;
+    long long psum[2] = {0, 0};
+    for (int l = lbase + lane; l <= lmax; l += 32) {
+      const int p = static_cast<int>(llrint(bval(l, col) * inv));
+      // signed base-256 digits, each in [-128, 127]
+      int d[4], r = p;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        d[k] = ((r + 128) & 255) - 128;
+        r = (r - d[k]) >> 8;
+      }
+      d[3] = r;
+      const int ll = l - lbase;
+      psum[ll & 1] += p;
+      const int jj = (ll & (kMC - 1)) >> 1;
+      unsigned char *tile = base + (long long)(ll / kMC) * BLK + kMC * CE + (ll & 1) * NP * kKB;
+#pragma unroll
+      for (int w = 2; w <= 6; ++w) {
+        uint32_t word = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (w - k >= 0 && w - k <= 3) word |= uint32_t(uint8_t(int8_t(d[w - k]))) << (8 * k);
+        const int row = col * kClasses + (w - 2);
+        *reinterpret_cast<uint32_t *>(tile + tile_off(row, 4 * jj)) = word;
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int o = 16; o; o >>= 1) psum[h] += __shfl_xor_sync(0xffffffffu, psum[h], o);
+    if (lane == 0) {
+      ep[col] = amax / (kQ * kQ);
+      ep[ncol + col] = 2147483648.0 * double(psum[0]);
+      ep[2 * ncol + col] = 2147483648.0 * double(psum[1]);
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// Epilogue: per ring pair, the exact int32 class sums of every (type, parity,
+// column) -> FP64 (sum_w D_w 2^(8w) - 2^31 sum p, times the column scale),
+// then the north/south phases.  TMEM is streamed 16 columns at a time and a
+// transform is finalised as soon as its columns are complete, so only a few
+// accumulators are live at once.
+// --------------------------------------------------------------------------
+// Exact int32 -> double without the conversion unit: 1.5*2^52 + (v + 2^31)
+// has an exact significand; subtracting 1.5*2^52 + 2^31 leaves v.
+__device__ __forceinline__ double i2d_exact(uint32_t v) {
+  return __hiloint2double(0x43380000, int(v ^ 0x80000000u)) - 6755401588539392.0;
+}
+
+template <class S>
+__device__ __forceinline__ void epilogue(uint32_t lane_base, const double *__restrict__ ep,
+                                         bool valid, bool has_s, int p, int m, int mhi, int spin,
+                                         double2 *__restrict__ phase, int ncm, int pcomp0,
+                                         int ms) {
+  constexpr int CPT = 2 * S::NCOMP;      // real columns per transform
+  constexpr int RPT = kClasses * CPT;    // B rows per transform
+  double R[S::T][2][S::NCOL];
+#pragma unroll
+  for (int q = 0; q < S::NPR; q += 16) {
+    uint32_t v[S::T][2][16];
+#pragma unroll
+    for (int t = 0; t < S::T; ++t)
+#pragma unroll
+      for (int par = 0; par < 2; ++par)
+        tmem_ld16(lane_base + uint32_t((t * 2 + par) * S::NP + q), v[t][par]);
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int row = q + i;
+      if (row < S::NPR) {
+        const int col = row / kClasses, w = row % kClasses + 2;
+        const double wt = double(1ull << (8 * w));
+#pragma unroll
+        for (int t = 0; t < S::T; ++t)
+#pragma unroll
+          for (int par = 0; par < 2; ++par) {
+            if (w == 2) R[t][par][col] = -ep[(1 + par) * S::NCOL + col];
+            R[t][par][col] = fma(i2d_exact(v[t][par][i]), wt, R[t][par][col]);
+          }
+      }
+    }
+    // transforms whose last row lies in this group are complete
+#pragma unroll
+    for (int j = 0; j < S::NB; ++j) {
+      const int last = (j + 1) * RPT - 1;
+      if (last < q || last >= q + 16) continue;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const double sc = ep[j * CPT + c];
+#pragma unroll
+        for (int t = 0; t < S::T; ++t)
+#pragma unroll
+          for (int par = 0; par < 2; ++par) R[t][par][j * CPT + c] *= sc;
+      }
+      if (!valid) continue;
+      if constexpr (S::T == 1) {
+        const long long row = ((long long)(p * ncm + pcomp0 + j) * 2) * ms;
+        const double er = R[0][0][2 * j], ei = R[0][0][2 * j + 1];
+        const double orr = R[0][1][2 * j], oi = R[0][1][2 * j + 1];
+        phase[row + m] = make_double2(er + orr, ei + oi);
+        if (has_s) phase[row + ms + m] = make_double2(er - orr, ei - oi);
+      } else {
+        const double flip = ((mhi - m + spin) & 1) ? -1.0 : 1.0;
+        constexpr int X = S::T - 1;
+        // columns of transform j: G re, G im, C re, C im
+        const double2 gwe = make_double2(R[0][0][4 * j], R[0][0][4 * j + 1]);
+        const double2 gwo = make_double2(R[0][1][4 * j], R[0][1][4 * j + 1]);
+        const double2 gxe = make_double2(R[X][0][4 * j], R[X][0][4 * j + 1]);
+        const double2 gxo = make_double2(R[X][1][4 * j], R[X][1][4 * j + 1]);
+        const double2 cwe = make_double2(R[0][0][4 * j + 2], R[0][0][4 * j + 3]);
+        const double2 cwo = make_double2(R[0][1][4 * j + 2], R[0][1][4 * j + 3]);
+        const double2 cxe = make_double2(R[X][0][4 * j + 2], R[X][0][4 * j + 3]);
+        const double2 cxo = make_double2(R[X][1][4 * j + 2], R[X][1][4 * j + 3]);
+        // q1 = Gwe + i Cxo, q2 = Gwo + i Cxe, u1 = Cwe - i Gxo, u2 = Cwo - i Gxe
+        const double2 q1 = make_double2(gwe.x - cxo.y, gwe.y + cxo.x);
+        const double2 q2 = make_double2(gwo.x - cxe.y, gwo.y + cxe.x);
+        const double2 u1 = make_double2(cwe.x + gxo.y, cwe.y - gxo.x);
+        const double2 u2 = make_double2(cwo.x + gxe.y, cwo.y - gxe.x);
+        const long long rq = ((long long)(p * ncm + pcomp0 + 2 * j) * 2) * ms;
+        const long long ru = ((long long)(p * ncm + pcomp0 + 2 * j + 1) * 2) * ms;
+        phase[rq + m] = make_double2(q1.x + q2.x, q1.y + q2.y);
+        phase[ru + m] = make_double2(u1.x + u2.x, u1.y + u2.y);
+        if (has_s) {
+          phase[rq + ms + m] = make_double2(flip * (q1.x - q2.x), flip * (q1.y - q2.y));
+          phase[ru + ms + m] = make_double2(flip * (u1.x - u2.x), flip * (u1.y - u2.y));
+        }
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// The synthesis kernel.
+// --------------------------------------------------------------------------
+template <class S>
+__global__ void __launch_bounds__(kThreads, S::MINB)
+mixed_synth_kernel(const int2 *__restrict__ items, const int *__restrict__ count,
+                   const double *__restrict__ cth, const double *__restrict__ sth,
+                   const int *__restrict__ nph_ring, const double *__restrict__ pre_v,
+                   const int *__restrict__ pre_e, int spin, const unsigned char *__restrict__ img,
+                   const long long *__restrict__ ioff, const double *__restrict__ epi, int lmax,
+                   double2 *__restrict__ phase, int ncm, int pcomp0, int ms,
+                   int *__restrict__ err) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ uint64_t full_b[kSB], full_a[kSA], done[kSA];
+  __shared__ uint32_t tslot;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int2 it = items[blockIdx.x];
+  const int m = it.x;
+  const int mhi = max(m, spin);
+  const int cnt = count[m];
+  const int nch = mhi <= lmax ? (lmax - mhi + kMC) / kMC : 0;
+  const unsigned char *img_m = img + ioff[m];
+  unsigned char *sB = sm;                         // kSB blocks
+  unsigned char *sA = sm + kSB * S::BLK;          // kSA x kRS x ATILES tiles
+
+  if (tid == 0) {
+    for (int i = 0; i < kSB; ++i) mbar_init(&full_b[i], 1);
+    for (int i = 0; i < kSA; ++i) {
+      mbar_init(&full_a[i], 4 * kRS);
+      mbar_init(&done[i], 1);
+    }
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(&tslot, S::NCOLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tslot;
+
+  if (warp == 4 * kRS) {
+    // ---------------- loader / MMA issuer (lane 0 issues) ----------------
+    if (nch > 0) {
+      if (lane == 0) {
+        const int npre = nch < kSB ? nch : kSB;
+        for (int c = 0; c < npre; ++c) {
+          mbar_arrive_tx(&full_b[c], S::BLK);
+          bulk_g2s(sB + c * S::BLK, img_m + (long long)c * S::BLK, S::BLK, &full_b[c]);
+        }
+      }
+      __syncwarp();
+      constexpr uint32_t idesc = make_idesc_i8(S::PS);
+      bool ok = true;
+      int issued = -1;
+      for (int c = 0; c < nch; ++c) {
+        const int sa = c % kSA, sb = c % kSB;
+        const bool ready =
+            mbar_wait(&full_a[sa], (c / kSA) & 1) && mbar_wait(&full_b[sb], (c / kSB) & 1);
+        if (!__all_sync(0xffffffffu, ready)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t a0 = smem_u32(sA + sa * kRS * S::ATILES * kTileBytes);
+          const uint32_t b0 = smem_u32(sB + sb * S::BLK + S::COEF);
+#pragma unroll
+          for (int rs = 0; rs < kRS; ++rs)
+#pragma unroll
+          for (int t = 0; t < S::T; ++t)
+#pragma unroll
+            for (int par = 0; par < 2; ++par) {
+              const uint32_t at = a0 + ((rs * S::T + t) * 2 + par) * kTileBytes;
+              const uint32_t bt = b0 + par * S::NP * kKB;
+#pragma unroll
+              for (int pc = 0; pc < S::NP / S::PS; ++pc)
+#pragma unroll
+                for (int s = 0; s < kKB / 32; ++s) {
+                  const uint32_t d =
+                      tmem + uint32_t(rs * S::TCOLS + (t * 2 + par) * S::NP + pc * S::PS);
+                  mma_i8(d, make_desc(at + s * 256, 128, 512),
+                         make_desc(bt + (pc * S::PS / 8) * 512 + s * 256, 128, 512), idesc,
+                         (c > 0 || s > 0) ? 1u : 0u);
+                }
+            }
+          mma_commit(&done[sa]);
+        }
+        __syncwarp();
+        issued = c;
+        // refill the block of chunk c-1 (its MMAs are normally complete by now)
+        const int cr = c - 1 + kSB;
+        if (c >= 1 && cr < nch) {
+          if (!__all_sync(0xffffffffu, mbar_wait(&done[(c - 1) % kSA], ((c - 1) / kSA) & 1))) {
+            ok = false;
+            break;
+          }
+          if (lane == 0) {
+            const int sr = cr % kSB;
+            mbar_arrive_tx(&full_b[sr], S::BLK);
+            bulk_g2s(sB + sr * S::BLK, img_m + (long long)cr * S::BLK, S::BLK, &full_b[sr]);
+          }
+          __syncwarp();
+        }
+      }
+      if (!ok) {
+        if (lane == 0) *reinterpret_cast<volatile int *>(err) = 1;
+        // let MMAs in flight drain (a commit tracks all earlier MMAs)
+        if (issued >= 0) mbar_wait(&done[issued % kSA], (issued / kSA) & 1);
+      }
+    }
+  } else {
+    // ---------------- producers: one ring pair per thread ----------------
+    const int rs = warp >> 2;                  // row set of this warp
+    const int row = tid & (kRows - 1);         // MMA row / TMEM lane
+    const int p = it.y * (kRS * kRows) + tid;
+    const bool valid = p < cnt;
+    const double x = valid ? cth[p] : 0.0;
+    bool ok = true;
+    double mu0, mu1, mm0 = 0.0, mm1 = 0.0;
+    int E, Em = 0;
+    bool act, live;
+    if constexpr (S::T == 1) {
+      XD sd = valid ? xd_pow(sth[p], m) : XD{0.0, 0};
+      sd = xd_norm(sd.v * ((m & 1) ? -pre_v[m] : pre_v[m]), sd.e);
+      mu0 = 0.0;
+      mu1 = sd.v;
+      E = sd.e;
+      live = valid && sd.v != 0.0;
+      act = live && E >= -kSwitchExp;
+      if (act) mu1 = ldexp(mu1, E);
+    } else {
+      live = spin_start(valid, x, valid ? sth[p] : 0.0, m, spin, pre_v[m], pre_e[m], mu0, mu1,
+                        mm0, mm1, E, Em, act);
+    }
+    for (int c = 0; c < nch; ++c) {
+      const int sa = c % kSA, sb = c % kSB;
+      const bool w1 = mbar_wait(&full_b[sb], (c / kSB) & 1);
+      const bool w2 = c < kSA || mbar_wait(&done[sa], ((c / kSA) - 1) & 1);
+      if (!__all_sync(0xffffffffu, w1 && w2)) {
+        ok = false;
+        break;
+      }
+      unsigned char *at = sA + (sa * kRS + rs) * S::ATILES * kTileBytes;
+      uint32_t u[S::T][2][kLP];
+      const uint32_t cf = smem_u32(sB + sb * S::BLK);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {  // two blocks of 16 l-steps
+        const bool all = __all_sync(0xffffffffu, act);
+        if constexpr (S::T == 1) {
+          if (all)
+            steps16_s0<true>(cf + h * 16 * S::CE, x, act, mu0, mu1, &u[0][0][8 * h],
+                             &u[0][1][8 * h]);
+          else
+            steps16_s0<false>(cf + h * 16 * S::CE, x, act, mu0, mu1, &u[0][0][8 * h],
+                              &u[0][1][8 * h]);
+        } else {
+#pragma unroll
+          for (int g = 0; g < 2; ++g) {
+            const uint32_t cg = cf + (h * 16 + 8 * g) * S::CE;
+            const int o = 8 * h + 4 * g;
+            if (all)
+              steps8_sp<true>(cg, x, act, mu0, mu1, mm0, mm1, &u[0][0][o], &u[S::T - 1][0][o],
+                              &u[0][1][o], &u[S::T - 1][1][o]);
+            else
+              steps8_sp<false>(cg, x, act, mu0, mu1, mm0, mm1, &u[0][0][o], &u[S::T - 1][0][o],
+                               &u[0][1][o], &u[S::T - 1][1][o]);
+          }
+        }
+        // every 16 l-steps: bookkeeping of rings still in the scaled regime
+        if constexpr (S::T == 1) {
+          if (live && !act) {
+            live = renorm_pair(mu1, mu0, E);
+            if (live && E >= -kSwitchExp) {
+              mu1 = ldexp(mu1, E);
+              mu0 = ldexp(mu0, E);
+              act = true;
+            }
+          }
+        } else {
+          spin_renorm(live, act, mu0, mu1, mm0, mm1, E, Em);
+        }
+      }
+      // this thread's row of every A tile: 64 bytes = 4 x 16
+      const uint32_t at32 = smem_u32(at);
+#pragma unroll
+      for (int t = 0; t < S::T; ++t)
+#pragma unroll
+        for (int par = 0; par < 2; ++par)
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            sts_u32x4(at32 + (t * 2 + par) * kTileBytes + tile_off(row, 16 * q),
+                      u[t][par][4 * q], u[t][par][4 * q + 1], u[t][par][4 * q + 2],
+                      u[t][par][4 * q + 3]);
+      fence_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full_a[sa]);
+    }
+    // epilogue: exact int32 class sums -> FP64 -> phase
+    if (ok && nch > 0) {
+      const int cl = nch - 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(&done[cl % kSA], (cl / kSA) & 1))) ok = false;
+    }
+    if (!ok) {
+      if (lane == 0) *reinterpret_cast<volatile int *>(err) = 1;
+    } else if (nch > 0) {
+      tc_fence_after();
+      epilogue<S>(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(rs * S::TCOLS),
+                  epi + (long long)m * 3 * S::NCOL, valid,
+                  valid ? nph_ring[2 * p + 1] > 0 : false, p, m, mhi, spin, phase, ncm, pcomp0,
+                  ms);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, S::NCOLS);
+  }
+}
+
+template <class S>
+void launch_shape(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp, const double2 *A,
+                  int ncA, int t0, double2 *phase, int ncm, int *d_err, cudaStream_t st) {
+  const int mmax = job.mmax, lmax = job.lmax, spin = job.spin;
+  std::vector<long long> ioff(mmax + 1);
+  long long tot = 0;
+  for (int m = 0; m <= mmax; ++m) {
+    ioff[m] = tot;
+    const int lbase = m > spin ? m : spin;
+    if (lbase <= lmax) tot += (long long)((lmax - lbase + kMC) / kMC) * S::BLK;
+  }
+  if (tot == 0) return;
+  unsigned char *img = nullptr;
+  long long *d_ioff = nullptr;
+  double *epi = nullptr;
+  const size_t epi_bytes = sizeof(double) * 3 * S::NCOL * (mmax + 1);
+  SHT_CUDA(cudaMallocAsync(&img, size_t(tot), st));
+  SHT_CUDA(cudaMallocAsync(&d_ioff, sizeof(long long) * (mmax + 1), st));
+  SHT_CUDA(cudaMallocAsync(&epi, epi_bytes, st));
+  SHT_CUDA(cudaMemcpyAsync(d_ioff, ioff.data(), sizeof(long long) * (mmax + 1),
+                           cudaMemcpyHostToDevice, st));
+  SHT_CUDA(cudaMemsetAsync(img, 0, size_t(tot), st));
+  SHT_CUDA(cudaMemsetAsync(epi, 0, epi_bytes, st));
+  {
+    ProfScope ps("mixed_image", st);
+    mixed_image_kernel<<<mmax + 1, 256, 0, st>>>(
+        lmax, spin, S::NCOL, S::NCOMP, S::NP, S::CE, S::BLK, cp.d_moff, cp.alpha, cp.beta,
+        cp.cfac, d_ioff, A, ncA, t0 * S::NCOMP, img, epi);
+    SHT_CUDA(cudaGetLastError());
+  }
+  {
+    ProfScope ps("legendre_synth", st);
+    auto k = mixed_synth_kernel<S>;
+    SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+    k<<<int(gp.mixed_items.size()), kThreads, S::SMEM, st>>>(
+        gp.mitems, gp.count, gp.cth, gp.sth, gp.nph, cp.seed, cp.seed_exp, spin, img, d_ioff,
+        epi, lmax, phase, ncm, t0 * S::NCOMP, mmax + 1, d_err);
+    SHT_CUDA(cudaGetLastError());
+  }
+  SHT_CUDA(cudaFreeAsync(img, st));
+  SHT_CUDA(cudaFreeAsync(d_ioff, st));
+  SHT_CUDA(cudaFreeAsync(epi, st));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launcher: staged FP64 a_lm (A, as for the FP64 path) -> image -> kernel,
+// in groups of up to 6 (spin 0) or 3 (spin > 0) transforms.
+// ---------------------------------------------------------------------------
+bool mixed_synth_supported(const JobDesc &job) {
+  return job.type == SHARP_ALM2MAP && job.ntrans >= 1;
+}
+
+// Largest number of transforms per launch (SHARP_B200_MIXED_GROUP, default
+// 6 for spin 0 and 3 for spin > 0; values above those are clamped).
+int mixed_group_cap() {
+  static int cap = [] {
+    const char *e = getenv("SHARP_B200_MIXED_GROUP");
+    const int v = e ? atoi(e) : 0;
+    return v > 0 ? v : 1 << 30;
+  }();
+  return cap;
+}
+
+void launch_mixed_synth(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
+                        const double2 *A, int ncA, double2 *phase, int ncm, int *d_err,
+                        cudaStream_t st) {
+  if (gp.mixed_items.empty()) return;  // no ring pair has an active m
+  for (int t0 = 0; t0 < job.ntrans;) {
+    const int left = std::min(job.ntrans - t0, mixed_group_cap());
+    int nb;
+#define SHT_MX(TV, CV, NBV) \
+  launch_shape<Shape<TV, CV, NBV>>(job, gp, cp, A, ncA, t0, phase, ncm, d_err, st)
+    if (job.spin == 0) {
+      nb = left >= 12 ? 12 : std::min(left, 6);
+      switch (nb) {
+        case 12: SHT_MX(1, 1, 12); break;
+        case 6: SHT_MX(1, 1, 6); break;
+        case 5: SHT_MX(1, 1, 5); break;
+        case 4: SHT_MX(1, 1, 4); break;
+        case 3: SHT_MX(1, 1, 3); break;
+        case 2: SHT_MX(1, 1, 2); break;
+        default: SHT_MX(1, 1, 1); break;
+      }
+    } else {
+      nb = std::min(left, 3);
+      switch (nb) {
+        case 3: SHT_MX(2, 2, 3); break;
+        case 2: SHT_MX(2, 2, 2); break;
+        default: SHT_MX(2, 2, 1); break;
+      }
+    }
+#undef SHT_MX
+    t0 += nb;
+  }
+}
+
+}  // namespace sht
