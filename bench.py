@@ -3,15 +3,24 @@
 workload: alm2map + map2alm round trips of a temperature+polarisation set
 (one spin-0 job T and one spin-2 job E,B -> Q,U per direction, as
 Healpix_cxx alm2map_pol / map2alm_pol do) on a HEALPix Nside=2048 map with
-lmax = mmax = 4096, FP64.
+lmax = mmax = 4096.
 
-One step = T+QU alm2map followed by T+QU map2alm.  ``value`` is round trips
-per second over all ranks with inputs resident in HBM; ``e2e`` is the same
-metric through the C ABI (sharp_execute) with pinned host buffers, so every
-step includes the host<->device copies.  N>1 runs independent replicas (the
-transform does not shard across GPUs in this workload).
+Two forms are measured in the same run:
+  * mixed (headline): a batch of B independent T+QU sets per step, every
+    sharp_execute job with ntrans = B and SHARP_MIXED (exact-integer
+    tensor-core Legendre contraction where the library has one, FP64
+    elsewhere).  value = round trips (sets) per second over all ranks; the
+    line carries the relative L2 error of the batch's outputs against the
+    FP64 path on the same inputs.
+  * fp64: the plain FP64 drop-in, one set per step (ntrans = 1).
+One step = T+QU alm2map followed by T+QU map2alm for each set of the step.
+``value`` has the inputs resident in HBM; ``e2e`` is the same metric through
+the C ABI (sharp_execute) with pinned host buffers, so every step includes
+the host<->device copies.  N>1 runs independent replicas (the transform does
+not shard across GPUs in this workload).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+                    [--form mixed|fp64] [--impl reference]
 """
 from __future__ import annotations
 
@@ -42,7 +51,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nside", type=int, default=2048)
     ap.add_argument("--lmax", type=int, default=4096)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
+                    help="headline form: batched SHARP_MIXED or the FP64 drop-in")
+    ap.add_argument("--batch", type=int, default=12, help="T+QU sets per step (mixed form)")
+    ap.add_argument("--fp64-steps", type=int, default=4,
+                    help="timed steps of the FP64 drop-in companion measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
                     help="run warm-up and timed steps only (for ncu launch lists)")
@@ -228,6 +242,87 @@ def cpu_baseline(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+FAMILIES = ("legendre_synth", "legendre_anal", "ring_synth", "ring_anal", "stage_alm",
+            "scatter_alm", "mixed_image")
+
+
+class Sets:
+    """B independent T+QU sets resident on the device: a_lm inputs, maps,
+    round-trip a_lm outputs (float64 views of complex128 a_lm)."""
+
+    def __init__(self, sb, torch, np, dev, lmax, npix, nalm, count, seed0):
+        self.count = count
+        self.host = [inputs(lmax, seed=seed0 + i) for i in range(count)]
+
+        def dalm(x):
+            return torch.from_numpy(x.view(np.float64).copy()).to(dev)
+
+        self.a = [[dalm(x) for x in h] for h in self.host]           # (t, e, b)
+        self.m = [[torch.zeros(npix, dtype=torch.float64, device=dev) for _ in range(3)]
+                  for _ in range(count)]                               # (T, Q, U)
+        self.o = [[torch.zeros(2 * nalm, dtype=torch.float64, device=dev) for _ in range(3)]
+                  for _ in range(count)]
+
+    def step(self, sb, geom, ainfo, n, flags, ops=None):
+        r = range(n)
+        ops = {} if ops is None else ops
+        ops["s0_synth"] = sb.execute_device(sb.SHARP_ALM2MAP, 0, [self.a[i][0] for i in r],
+                                            [self.m[i][0] for i in r], geom, ainfo, n, flags)
+        ops["s2_synth"] = sb.execute_device(
+            sb.SHARP_ALM2MAP, 2, [x for i in r for x in self.a[i][1:]],
+            [x for i in r for x in self.m[i][1:]], geom, ainfo, n, flags)
+        ops["s0_anal"] = sb.execute_device(sb.SHARP_MAP2ALM, 0, [self.o[i][0] for i in r],
+                                           [self.m[i][0] for i in r], geom, ainfo, n, flags)
+        ops["s2_anal"] = sb.execute_device(
+            sb.SHARP_MAP2ALM, 2, [x for i in r for x in self.o[i][1:]],
+            [x for i in r for x in self.m[i][1:]], geom, ainfo, n, flags)
+        return ops
+
+
+def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
+    """Device time per step (CUDA events on the launching stream, barrier +
+    synchronize on both sides), launch count and per-family kernel time."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.sharp_b200_kernel_launches()
+    lib.sharp_b200_profile(1)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if clk:
+        clk.__enter__()
+    ev0.record(stream)
+    for _ in range(steps):
+        fn()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__()
+    if dist:
+        dist.barrier()
+    launches = lib.sharp_b200_kernel_launches() - l0
+    fam = {}
+    for name in FAMILIES:
+        n = C.c_ulonglong(0)
+        ms = lib.sharp_b200_profile_ms(name.encode(), C.byref(n))
+        if n.value:
+            fam[name] = (ms, n.value)
+    lib.sharp_b200_profile(0)
+    step_s = ev0.elapsed_time(ev1) * 1e-3 / steps
+    if dist:
+        tt = torch.tensor([step_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step_s = float(tt.item())
+    return step_s, launches, fam
+
+
+def rel(torch, a, b):
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -254,83 +349,70 @@ def main():
     nalm = sb.nalm_triangular(lmax)
     geom = sb.Geometry.healpix(nside)
     ainfo = sb.AlmInfo.triangular(lmax)
-    t, e, b = inputs(lmax, seed=7 + rank)
     dev = torch.device("cuda", local)
-
-    def dalm(x):
-        return torch.from_numpy(x.view(np.float64).copy()).to(dev)
-
-    at, ae, ab = dalm(t), dalm(e), dalm(b)
-    mt, mq, mu = (torch.zeros(npix, dtype=torch.float64, device=dev) for _ in range(3))
-    ot, oe, ob = (torch.zeros(2 * nalm, dtype=torch.float64, device=dev) for _ in range(3))
+    mixed = args.form == "mixed"
+    B = max(1, args.batch) if mixed else 1
     DP = sb.SHARP_DP
-    flops = {}
-
-    def step():
-        flops["s0_synth"] = sb.execute_device(sb.SHARP_ALM2MAP, 0, [at], [mt], geom, ainfo, 1, DP)
-        flops["s2_synth"] = sb.execute_device(sb.SHARP_ALM2MAP, 2, [ae, ab], [mq, mu], geom, ainfo,
-                                              1, DP)
-        flops["s0_anal"] = sb.execute_device(sb.SHARP_MAP2ALM, 0, [ot], [mt], geom, ainfo, 1, DP)
-        flops["s2_anal"] = sb.execute_device(sb.SHARP_MAP2ALM, 2, [oe, ob], [mq, mu], geom, ainfo,
-                                             1, DP)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+    flags = DP | (sb.SHARP_MIXED if mixed else 0)
+    sets = Sets(sb, torch, np, dev, lmax, npix, nalm, B, seed0=7 + 1000 * rank)
 
     lib = sb.lib()
     lib.sharp_b200_kernel_launches.restype = C.c_ulonglong
     lib.sharp_b200_profile_ms.restype = C.c_double
     lib.sharp_b200_profile_ms.argtypes = [C.c_char_p, C.POINTER(C.c_ulonglong)]
     stream = torch.cuda.current_stream()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = lib.sharp_b200_kernel_launches()
-    lib.sharp_b200_profile(1)
-    with ClockSampler(local) as clk:
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    launches = lib.sharp_b200_kernel_launches() - launches0
-    step_s = ev0.elapsed_time(ev1) * 1e-3 / args.steps
-    fam = {}
-    for name in ("legendre_synth", "legendre_anal", "ring_synth", "ring_anal", "stage_alm",
-                 "scatter_alm"):
-        n = C.c_ulonglong(0)
-        ms = lib.sharp_b200_profile_ms(name.encode(), C.byref(n))
-        fam[name] = (ms, n.value)
-    lib.sharp_b200_profile(0)
-    if dist:
-        tt = torch.tensor([step_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_s = float(tt.item())
+
+    ops = {}
+    clk = ClockSampler(local)
+    step_s, launches, fam = timed(torch, lib, stream,
+                                  lambda: sets.step(sb, geom, ainfo, B, flags, ops),
+                                  args.steps, args.warmup, dist, clk)
     if args.profile_only:
         if dist:
             dist.destroy_process_group()
         return
-    value = world / step_s
+    value = world * B / step_s
+    head_out = [x.clone() for x in sets.m[0] + sets.o[0]]
 
-    # end-to-end through sharp_execute with pinned host buffers
-    def pinned(shape, dtype):
-        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+    # the FP64 drop-in on set 0 (ntrans = 1): companion number and the error
+    # reference for the mixed outputs
+    fp64_ops = {}
+    fp64_s, fp64_launches, fp64_fam = timed(
+        torch, lib, stream, lambda: sets.step(sb, geom, ainfo, 1, DP, fp64_ops),
+        args.fp64_steps if mixed else args.steps, 2, dist)
+    ref_out = sets.m[0] + sets.o[0]
+    err = {"maps": max(rel(torch, head_out[i], ref_out[i]) for i in range(3)),
+           "alms": max(rel(torch, head_out[i], ref_out[i]) for i in range(3, 6))}
 
-    ht, he, hb = (pinned(nalm, torch.complex128) for _ in range(3))
-    ht[:], he[:], hb[:] = t, e, b
-    hmt, hmq, hmu = (pinned(npix, torch.float64) for _ in range(3))
-    hot, hoe, hob = (pinned(nalm, torch.complex128) for _ in range(3))
+    # end-to-end through sharp_execute with pinned host buffers, the same
+    # batch and flags as the headline
+    def pinned(n, dtype):
+        return torch.empty(n, dtype=dtype, pin_memory=True).numpy()
+
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except ImportError:
+        avail = 0
+    need = B * 3 * (npix * 8 + 2 * nalm * 16)
+    nh = B if avail > 4 * need else 1   # distinct host buffers when host memory allows
+    h_alm = [[pinned(nalm, torch.complex128) for _ in range(3)] for _ in range(nh)]
+    h_map = [[pinned(npix, torch.float64) for _ in range(3)] for _ in range(nh)]
+    h_out = [[pinned(nalm, torch.complex128) for _ in range(3)] for _ in range(nh)]
+    for i in range(nh):
+        for j in range(3):
+            h_alm[i][j][:] = sets.host[i][j]
+    hs = [i % nh for i in range(B)]
 
     def host_step():
-        sb.execute(sb.SHARP_ALM2MAP, 0, [ht], [hmt], geom, ainfo, 1, DP)
-        sb.execute(sb.SHARP_ALM2MAP, 2, [he, hb], [hmq, hmu], geom, ainfo, 1, DP)
-        sb.execute(sb.SHARP_MAP2ALM, 0, [hot], [hmt], geom, ainfo, 1, DP)
-        sb.execute(sb.SHARP_MAP2ALM, 2, [hoe, hob], [hmq, hmu], geom, ainfo, 1, DP)
+        sb.execute(sb.SHARP_ALM2MAP, 0, [h_alm[i][0] for i in hs], [h_map[i][0] for i in hs],
+                   geom, ainfo, B, flags)
+        sb.execute(sb.SHARP_ALM2MAP, 2, [x for i in hs for x in h_alm[i][1:]],
+                   [x for i in hs for x in h_map[i][1:]], geom, ainfo, B, flags)
+        sb.execute(sb.SHARP_MAP2ALM, 0, [h_out[i][0] for i in hs], [h_map[i][0] for i in hs],
+                   geom, ainfo, B, flags)
+        sb.execute(sb.SHARP_MAP2ALM, 2, [x for i in hs for x in h_out[i][1:]],
+                   [x for i in hs for x in h_map[i][1:]], geom, ainfo, B, flags)
 
     host_step()
     if dist:
@@ -343,43 +425,43 @@ def main():
         tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
-    h2d = 3 * nalm * 16 + 3 * npix * 8
-    d2h = 3 * npix * 8 + 3 * nalm * 16
+    h2d = B * (3 * nalm * 16 + 3 * npix * 8)
+    d2h = B * (3 * npix * 8 + 3 * nalm * 16)
+    t_in = sets.host[0][0]
+    api_err = float(np.linalg.norm(head_out[3].cpu().numpy().view(np.complex128) - h_out[0][0])
+                    / np.linalg.norm(h_out[0][0]))
+    rt_err = float(np.linalg.norm(h_out[0][0] - t_in) / np.linalg.norm(t_in))
 
-    # correctness of this run's output (round trip without iteration, and
-    # GPU-vs-host-API agreement)
-    rt_err = float(np.linalg.norm(hot - t) / np.linalg.norm(t))
-    api_err = float(np.linalg.norm(ot.cpu().numpy().view(np.complex128) - hot) / np.linalg.norm(hot))
-
-    # roofline of the dominant kernel family (FP64 FMA pipe bound)
-    dom = max(("legendre_synth", "legendre_anal"), key=lambda k: fam[k][0])
+    # roofline of the dominant kernel family
+    dom = max(("legendre_synth", "legendre_anal"), key=lambda k: fam.get(k, (0, 0))[0])
     dom_ms, dom_n = fam[dom]
-    dom_flops = (flops["s0_synth"] + flops["s2_synth"]) if dom == "legendre_synth" else \
-        (flops["s0_anal"] + flops["s2_anal"])
-    achieved = dom_flops * args.steps / (dom_ms * 1e-3) / 1e12
-    peak = fp64_gemm_peak(torch)
-    traffic = dram_traffic_from_profiles()
-    share = {k: round(v[0] / max(1e-9, sum(x[0] for x in fam.values())), 4) for k, v in fam.items()}
+    roof = roofline(dom, dom_ms, dom_n, ops, B, mixed, args.steps, fp64_gemm_peak(torch))
+    tot = sum(v[0] for v in fam.values())
+    share = {k: round(v[0] / max(1e-9, tot), 4) for k, v in fam.items()}
 
+    form = (f"mixed: batch of {B} sets per step, SHARP_MIXED (int8 tensor-core Legendre "
+            f"synthesis; analysis FP64)" if mixed else "fp64 drop-in, one set per step")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+i8" if mixed else "f64", "data": "synthetic",
             "config": {"workload": f"T+QU alm2map+map2alm, HEALPix Nside {nside}, "
-                                   f"lmax=mmax={lmax}, spin 0+2, FP64 drop-in",
-                       "nside": nside, "lmax": lmax, "form": "fp64",
+                                   f"lmax=mmax={lmax}, spin 0+2, {form}",
+                       "nside": nside, "lmax": lmax, "form": args.form, "batch": B,
                        "alm": "a_lm ~ C_l = (l+1)^-2 exp(-l(l+1) sigma^2), sigma 5', E 0.1, B 0.01",
                        "l2": "inputs larger than L2 (each map 403 MB, each a_lm 134 MB)",
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+            "rel_err_vs_fp64": err,
+            "fp64_dropin": {"value": world / fp64_s, "unit": UNIT, "ms_per_step": fp64_s * 1e3,
+                            "kernel_ms_per_step": {k: round(v[0] / (args.fp64_steps if mixed
+                                                                      else args.steps), 3)
+                                                   for k, v in fp64_fam.items()}},
+            "e2e": {"value": world * B / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "host_buffers": "distinct" if nh == B else "shared"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak,
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-                         "flops_per_launch": dom_flops / 2, "ms_per_launch": dom_ms / max(dom_n, 1),
-                         "traffic": traffic},
+            "roofline": roof,
             "kernel_time_share": share,
+            "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in fam.items()},
             "clocks": clk.summary(),
             "check": {"round_trip_rel_err_no_iteration": rt_err, "device_vs_host_api": api_err}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -388,6 +470,33 @@ def main():
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def roofline(dom, dom_ms, dom_n, ops, B, mixed, steps, peak):
+    """Achieved FP64 rate of the dominant Legendre family against the
+    measured DGEMM peak.  FP64 kernels: the reference's operation count
+    (sharp_execute's opcnt).  Mixed synthesis: the FP64 work its producers
+    execute per (ring pair, l): recurrence plus quantisation, 5 flops at spin
+    0 and 12 at spin 2 (the contraction itself runs on the int8 tensor
+    pipe)."""
+    if dom == "legendre_synth":
+        if mixed:
+            v0 = ops["s0_synth"] / (4 + 4 * B)      # (ring pair, l) values of the spin-0 job
+            v2 = ops["s2_synth"] / (12 + 16 * B)
+            flops = 5 * v0 + 12 * v2
+            what = "mixed synthesis producer FP64 work (recurrence + quantisation)"
+        else:
+            flops = ops["s0_synth"] + ops["s2_synth"]
+            what = "reference operation count"
+    else:
+        flops = ops["s0_anal"] + ops["s2_anal"]
+        what = "reference operation count"
+    achieved = flops * steps / (dom_ms * 1e-3) / 1e12
+    return {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "work": what,
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+            "flops_per_step": flops, "ms_per_launch": dom_ms / max(dom_n, 1),
+            "traffic": dram_traffic_from_profiles()}
 
 
 if __name__ == "__main__":
