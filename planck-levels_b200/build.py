@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
               "-I", os.path.join(ROOT, "include"), "-I", CSRC] + ARCH
-SOURCES = ["sht_host.cc", "sht_execute.cu", "sht_legendre.cu", "sht_ring.cu", "sht_profile.cu", "sht_noalloc.cu", "sht_mixed.cu"]
+SOURCES = ["sht_host.cc", "sht_execute.cu", "sht_legendre.cu", "sht_ring.cu", "sht_profile.cu", "sht_noalloc.cu", "sht_mixed.cu", "sht_mixed_anal.cu"]
 
 
 def nvcc() -> str:

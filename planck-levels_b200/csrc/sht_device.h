@@ -83,6 +83,7 @@ struct CoefPlan {
   double *cfac = nullptr;            // c_l
   double *seed = nullptr;            // spin 0: mfac[m]; spin>0: prefac mantissa
   int *seed_exp = nullptr;           // spin>0: prefac exponent (base 2)
+  double2 *mx_coef = nullptr;        // mixed analysis: (alpha_l, c_l 2^30 / b_l), lazily built
   CoefPlan() = default;
   CoefPlan(const CoefPlan &) = delete;
   CoefPlan &operator=(const CoefPlan &) = delete;
@@ -120,6 +121,10 @@ bool mixed_synth_supported(const JobDesc &job);
 void launch_mixed_synth(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
                         const double2 *A, int ncA, double2 *phase, int ncm, int *d_err,
                         cudaStream_t st);
+bool mixed_anal_supported(const JobDesc &job);
+void launch_mixed_anal(const JobDesc &job, const GeomPlan &gp, CoefPlan &cp,
+                       const double2 *phase, int ncm, double2 *Aout, int ncA, int *d_err,
+                       cudaStream_t st);
 
 // Kernel launchers (sht_legendre.cu)
 void launch_coef_tables(CoefPlan &cp, cudaStream_t st);

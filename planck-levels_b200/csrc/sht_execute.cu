@@ -668,11 +668,17 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
                         nmapptr, phase, ncm, st);
     DevBuf d_Aout(sizeof(double2) * size_t(cp->total) * ncA, st);
     SHT_CUDA(cudaMemsetAsync(d_Aout.p, 0, sizeof(double2) * size_t(cp->total) * ncA, st));
-    for (int t0 = 0; t0 < ntrans;) {
-      const int nt = group(ntrans - t0, ntmax_anal);
-      launch_legendre_anal(job, *gp, *cp, phase, ncm, t0 * job.nmaps, nt, d_Aout.as<double>(),
-                           ncA, t0 * job.nalm, st);
-      t0 += nt;
+    if ((flags & SHARP_MIXED) && mixed_anal_supported(job)) {
+      int *d_err = nullptr;
+      tc_error_word(&d_err);
+      launch_mixed_anal(job, *gp, *cp, phase, ncm, d_Aout.as<double2>(), ncA, d_err, st);
+    } else {
+      for (int t0 = 0; t0 < ntrans;) {
+        const int nt = group(ntrans - t0, ntmax_anal);
+        launch_legendre_anal(job, *gp, *cp, phase, ncm, t0 * job.nmaps, nt,
+                             d_Aout.as<double>(), ncA, t0 * job.nalm, st);
+        t0 += nt;
+      }
     }
     launch_scatter_alm(job, *ap, alm_lo, *cp, d_norm.as<double>(), d_Aout.as<double>(), ncA,
                        reinterpret_cast<void *const *>(d_almptr.p), nalmptr, st);
@@ -721,6 +727,7 @@ GeomPlan::~GeomPlan() {
 CoefPlan::~CoefPlan() {
   dev_free(d_moff); dev_free(alpha); dev_free(beta); dev_free(cfac); dev_free(seed);
   dev_free(seed_exp);
+  dev_free(mx_coef);
 }
 AlmPlan::~AlmPlan() { dev_free(mvstart); }
 

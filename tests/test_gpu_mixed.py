@@ -122,3 +122,69 @@ def test_mixed_device_entry_high_lmax():
     torch.cuda.synchronize()
     for x, y in zip(mmx, m64):
         assert rel_l2(x.cpu().numpy(), y.cpu().numpy()) < TOL
+
+
+# ---------------------------------------------------------------------------
+# map2alm with SHARP_MIXED (tensor-core analysis, spin 0)
+# ---------------------------------------------------------------------------
+def _anal_both(spec, lmax, mmax, ntrans, seed=0, flags=0, init=None):
+    g = _geom(spec)
+    a = sb.AlmInfo.triangular(lmax, mmax)
+    npix, nalm = g.npix(), sb.nalm_triangular(lmax, mmax)
+    rng = np.random.default_rng(seed)
+    maps = [rng.standard_normal(npix) for _ in range(ntrans)]
+    o64 = [np.zeros(nalm, np.complex128) if init is None else init[i].copy()
+           for i in range(ntrans)]
+    omx = [x.copy() for x in o64]
+    sb.execute(sb.SHARP_MAP2ALM, 0, o64, [x.copy() for x in maps], g, a, ntrans, DP | flags)
+    sb.execute(sb.SHARP_MAP2ALM, 0, omx, [x.copy() for x in maps], g, a, ntrans,
+               DP | MIXED | flags)
+    return o64, omx
+
+
+@pytest.mark.parametrize("ntrans", [1, 2, 3, 4, 5, 9])
+def test_mixed_analysis_healpix_batches(ntrans):
+    o64, omx = _anal_both(("healpix", 48), 96, 96, ntrans, seed=ntrans)
+    for x, y in zip(omx, o64):
+        assert rel_l2(x, y) < TOL
+
+
+@pytest.mark.parametrize("spec,lmax,mmax", [
+    (("gauss", 130, 259), 129, 129),
+    (("gauss", 64, 128), 63, 40),       # mmax < lmax
+    (("cc", 90, 171), 80, 80),          # poles on the grid
+    (("healpix", 128), 300, 300),       # lmax > 2 nside, several ring groups
+    (("healpix", 160), 200, 200),       # more than 256 ring pairs per m
+])
+def test_mixed_analysis_geometries(spec, lmax, mmax):
+    o64, omx = _anal_both(spec, lmax, mmax, 4, seed=11)
+    for x, y in zip(omx, o64):
+        assert rel_l2(x, y) < TOL
+
+
+def test_mixed_analysis_add_flag():
+    lmax = 64
+    rng = np.random.default_rng(5)
+    nalm = sb.nalm_triangular(lmax)
+    init = [rng.standard_normal(nalm) + 1j * rng.standard_normal(nalm) for _ in range(3)]
+    o64, omx = _anal_both(("healpix", 32), lmax, lmax, 3, seed=6, flags=sb.SHARP_ADD,
+                          init=init)
+    for x, y, z in zip(omx, o64, init):
+        assert rel_l2(x - z, y - z) < TOL
+
+
+def test_mixed_round_trip_against_reference():
+    import ref
+    if not ref.available():
+        pytest.skip("reference library not built (make -C oracle)")
+    nside, lmax = 64, 128
+    g, a = ref.healpix(nside), ref.triangular(lmax, lmax)
+    rng = np.random.default_rng(9)
+    maps = [rng.standard_normal(12 * nside * nside) for _ in range(4)]
+    out_ref = [np.zeros(sb.nalm_triangular(lmax), np.complex128) for _ in maps]
+    ref.execute(sb.SHARP_MAP2ALM, 0, out_ref, [x.copy() for x in maps], g, a, 4, DP)
+    gg, aa = sb.Geometry.healpix(nside), sb.AlmInfo.triangular(lmax, lmax)
+    out = [np.zeros_like(x) for x in out_ref]
+    sb.execute(sb.SHARP_MAP2ALM, 0, out, [x.copy() for x in maps], gg, aa, 4, DP | MIXED)
+    for x, y in zip(out, out_ref):
+        assert rel_l2(x, y) < TOL
