@@ -624,7 +624,11 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
   DevBuf d_phase(phase_bytes, st);
   double2 *phase = d_phase.as<double2>();
   const int ntmax_synth = (spin == 0 && !deriv) ? 4 : 2;
-  const int ntmax_anal = (spin == 0) ? 4 : 2;
+  // FP64 analysis: one transform per launch is fastest per transform (the
+  // per-thread phase factors of several transforms cost occupancy): at Nside
+  // 2048 / lmax 4096, spin 0 takes 14.1 ms at 1, 15.2 ms each at 4; spin 2
+  // takes 44.9 ms at 1, 54.1 ms each at 2.
+  const int ntmax_anal = 1;
   auto group = [&](int left, int ntmax) {
     int nt = 1;
     while (nt * 2 <= ntmax && nt * 2 <= left) nt *= 2;

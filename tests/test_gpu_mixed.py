@@ -188,3 +188,35 @@ def test_mixed_round_trip_against_reference():
     sb.execute(sb.SHARP_MAP2ALM, 0, out, [x.copy() for x in maps], gg, aa, 4, DP | MIXED)
     for x, y in zip(out, out_ref):
         assert rel_l2(x, y) < TOL
+
+
+def _anal_spin_both(spec, lmax, mmax, ntrans, spin, seed=0):
+    g = _geom(spec)
+    a = sb.AlmInfo.triangular(lmax, mmax)
+    npix, nalm = g.npix(), sb.nalm_triangular(lmax, mmax)
+    rng = np.random.default_rng(seed)
+    maps = [rng.standard_normal(npix) for _ in range(2 * ntrans)]
+    o64 = [np.zeros(nalm, np.complex128) for _ in range(2 * ntrans)]
+    omx = [x.copy() for x in o64]
+    sb.execute(sb.SHARP_MAP2ALM, spin, o64, [x.copy() for x in maps], g, a, ntrans, DP)
+    sb.execute(sb.SHARP_MAP2ALM, spin, omx, [x.copy() for x in maps], g, a, ntrans, DP | MIXED)
+    return o64, omx
+
+
+@pytest.mark.parametrize("spin,ntrans", [(1, 1), (2, 1), (2, 2), (2, 3), (3, 2)])
+def test_mixed_spin_analysis_batches(spin, ntrans):
+    o64, omx = _anal_spin_both(("healpix", 48), 96, 96, ntrans, spin, seed=spin + ntrans)
+    for x, y in zip(omx, o64):
+        assert rel_l2(x, y) < TOL
+
+
+@pytest.mark.parametrize("spec,lmax,mmax", [
+    (("gauss", 130, 259), 129, 129),
+    (("gauss", 64, 128), 63, 40),
+    (("cc", 90, 171), 80, 80),
+    (("healpix", 128), 300, 300),       # several 128-pair groups per m
+])
+def test_mixed_spin2_analysis_geometries(spec, lmax, mmax):
+    o64, omx = _anal_spin_both(spec, lmax, mmax, 2, 2, seed=21)
+    for x, y in zip(omx, o64):
+        assert rel_l2(x, y) < TOL
