@@ -85,6 +85,13 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.first = 0
+
+    def mark(self):
+        """Only samples taken after this call enter the summary (the sampler
+        is started before the warm-up: nvidia-smi's start-up stalls the GPU
+        for a moment and must not fall into the timed region)."""
+        self.first = len(self.lines)
 
     def __enter__(self):
         try:
@@ -110,7 +117,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.first:]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -282,6 +289,10 @@ class Sets:
 def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     """Device time per step (CUDA events on the launching stream, barrier +
     synchronize on both sides), launch count and per-family kernel time."""
+    if clk:
+        clk.__enter__()
+        time.sleep(2.0)   # let nvidia-smi finish starting before the warm-up ends
+    lib.sharp_b200_profile(1)   # warm-up runs with the same event instrumentation
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
@@ -289,15 +300,14 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
         dist.barrier()
     torch.cuda.synchronize()
     l0 = lib.sharp_b200_kernel_launches()
-    lib.sharp_b200_profile(1)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    lib.sharp_b200_profile(1)   # clears the warm-up spans
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     if clk:
-        clk.__enter__()
-    ev0.record(stream)
-    for _ in range(steps):
+        clk.mark()
+    evs[0].record(stream)
+    for i in range(steps):
         fn()
-    ev1.record(stream)
+        evs[i + 1].record(stream)
     torch.cuda.synchronize()
     if clk:
         clk.__exit__()
@@ -311,12 +321,13 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
         if n.value:
             fam[name] = (ms, n.value)
     lib.sharp_b200_profile(0)
-    step_s = ev0.elapsed_time(ev1) * 1e-3 / steps
+    step_s = evs[0].elapsed_time(evs[-1]) * 1e-3 / steps
+    per_step = [round(evs[i].elapsed_time(evs[i + 1]), 2) for i in range(steps)]
     if dist:
         tt = torch.tensor([step_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         step_s = float(tt.item())
-    return step_s, launches, fam
+    return step_s, launches, fam, per_step
 
 
 def rel(torch, a, b):
@@ -364,9 +375,9 @@ def main():
 
     ops = {}
     clk = ClockSampler(local)
-    step_s, launches, fam = timed(torch, lib, stream,
-                                  lambda: sets.step(sb, geom, ainfo, B, flags, ops),
-                                  args.steps, args.warmup, dist, clk)
+    step_s, launches, fam, per_step = timed(torch, lib, stream,
+                                            lambda: sets.step(sb, geom, ainfo, B, flags, ops),
+                                            args.steps, args.warmup, dist, clk)
     if args.profile_only:
         if dist:
             dist.destroy_process_group()
@@ -377,7 +388,7 @@ def main():
     # the FP64 drop-in on set 0 (ntrans = 1): companion number and the error
     # reference for the mixed outputs
     fp64_ops = {}
-    fp64_s, fp64_launches, fp64_fam = timed(
+    fp64_s, fp64_launches, fp64_fam, _ = timed(
         torch, lib, stream, lambda: sets.step(sb, geom, ainfo, 1, DP, fp64_ops),
         args.fp64_steps if mixed else args.steps, 2, dist)
     ref_out = sets.m[0] + sets.o[0]
@@ -462,6 +473,7 @@ def main():
             "roofline": roof,
             "kernel_time_share": share,
             "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in fam.items()},
+            "step_ms": per_step,
             "clocks": clk.summary(),
             "check": {"round_trip_rel_err_no_iteration": rt_err, "device_vs_host_api": api_err}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
