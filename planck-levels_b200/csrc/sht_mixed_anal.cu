@@ -137,16 +137,23 @@ __device__ __forceinline__ void flush_pair(uint32_t tmem, int f, int ntile, int 
                                            int warp, int lane) {
   const int k = warp & 3;
   const uint32_t base = tmem + (uint32_t(32 * k) << 16) + uint32_t((f & 1) * S::NP);
+  const int t = 2 * f + (lane >> 4);
+  const int l = l0 + t * kAM + 16 * k + (lane & 15);
+  const bool row = t < ntile && l <= lmax;
+  // the output entries and the row factor are fetched before the TMEM reads
+  double2 *out = Aout + (mo + (row ? l : l0)) * ncA + comp0;
+  double2 o[S::NCOL / 2];
+#pragma unroll
+  for (int j = 0; j < S::NCOL / 2; ++j) o[j] = row ? out[j] : make_double2(0.0, 0.0);
+  const double cq = !row ? 1.0 : S::SPIN ? __ldg(coef + 2 * (mo + l) + 1).x
+                                         : __ldg(coef + mo + l).y;
   uint32_t v[S::NP];
 #pragma unroll
   for (int q = 0; q < S::NP; q += 16) tmem_ld16(base + q, *reinterpret_cast<uint32_t(*)[16]>(v + q));
   tmem_ld_wait();
-  const int t = 2 * f + (lane >> 4);
-  const int l = l0 + t * kAM + 16 * k + (lane & 15);
-  if (t >= ntile || l > lmax) return;
+  if (!row) return;
   // the output is sum_p mu_l phi (the scatter applies c_l): lambda was
   // quantised as c_l mu_l 2^30 / b_l, so the row factor is b_l / c_l = 2^30 / cq_l
-  const double cq = S::SPIN ? __ldg(coef + 2 * (mo + l) + 1).x : __ldg(coef + mo + l).y;
   const double b = kQ / cq;
   const double sg = ((l - l0) & 1) ? -b : b;
   double R[S::NH];
@@ -158,13 +165,11 @@ __device__ __forceinline__ void flush_pair(uint32_t tmem, int f, int ntile, int 
     const double Pd = __longlong_as_double(P + 0x4338000000000000LL) - 6755399441055744.0;
     R[h] = (fma(i2d_exact(d[4]), 4294967296.0, Pd) - s_corr[h]) * s_fscale[h];
   }
-  double2 *out = Aout + (mo + l) * ncA + comp0;
 #pragma unroll
   for (int j = 0; j < S::NCOL / 2; ++j) {
-    double2 o = out[j];
-    o.x += b * R[2 * j] + sg * R[S::NCOL + 2 * j];
-    o.y += b * R[2 * j + 1] + sg * R[S::NCOL + 2 * j + 1];
-    out[j] = o;
+    o[j].x += b * R[2 * j] + sg * R[S::NCOL + 2 * j];
+    o[j].y += b * R[2 * j + 1] + sg * R[S::NCOL + 2 * j + 1];
+    out[j] = o[j];
   }
 }
 
@@ -431,14 +436,20 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
             double2 c[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) c[i] = lds_f64x2(cs + (16 * blk + i) * 16);
+            uint32_t u[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
               const double cq = (all || act) ? c[i].y : 0.0;
-              const int r = 16 * blk + i;
-              sts_u32(slice + (r >> 3) * 128 + (r & 7) * 16, quant(mu1, cq));
+              u[i] = quant(mu1, cq);
               const double nx = fma(c[i].x * x, mu1, -mu0);
               mu0 = mu1;
               mu1 = nx;
+            }
+            // stores after the steps: no store waits on its quantisation
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int r = 16 * blk + i;
+              sts_u32(slice + (r >> 3) * 128 + (r & 7) * 16, u[i]);
             }
           } else {
 #pragma unroll
@@ -451,17 +462,23 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
                 ab[i] = lds_f64x2(cs + li * 32);
                 cq[i] = lds_f64x2(cs + li * 32 + 16).x;
               }
+              uint32_t up[8], um[8];
 #pragma unroll
               for (int i = 0; i < 8; ++i) {
                 const double q = (all || act) ? cq[i] : 0.0;
-                const int r = 16 * blk + 8 * h8 + i;
-                sts_u32x2(slice + (r >> 3) * 128 + (r & 7) * 16, quant(mu1, q), quant(mm1, q));
+                up[i] = quant(mu1, q);
+                um[i] = quant(mm1, q);
                 const double np_ = fma(fma(ab[i].x, x, -ab[i].y), mu1, -mu0);
                 const double nm_ = fma(fma(ab[i].x, x, ab[i].y), mm1, -mm0);
                 mu0 = mu1;
                 mu1 = np_;
                 mm0 = mm1;
                 mm1 = nm_;
+              }
+#pragma unroll
+              for (int i = 0; i < 8; ++i) {
+                const int r = 16 * blk + 8 * h8 + i;
+                sts_u32x2(slice + (r >> 3) * 128 + (r & 7) * 16, up[i], um[i]);
               }
             }
           }
