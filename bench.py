@@ -159,12 +159,14 @@ def fp64_gemm_peak(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def dram_traffic_from_profiles():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+def dram_traffic_from_profiles(family):
+    """Per-launch DRAM bytes of a kernel family from its committed ncu
     summary (line 'dram_bytes_per_launch: <int>'), else None."""
-    path = os.path.join(ROOT, "profiles", "legendre_synth_nside2048.txt")
+    name = TRAFFIC_FILE.get(family)
+    if not name:
+        return None
     try:
-        for ln in open(path):
+        for ln in open(os.path.join(ROOT, "profiles", name)):
             if ln.startswith("dram_bytes_per_launch:"):
                 return int(float(ln.split(":")[1]))
     except OSError:
@@ -249,8 +251,17 @@ def cpu_baseline(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-FAMILIES = ("legendre_synth", "legendre_anal", "ring_synth", "ring_anal", "stage_alm",
+FAMILIES = ("legendre_synth", "legendre_anal", "mixed_synth_spin0", "mixed_synth_spin",
+            "mixed_anal_spin0", "mixed_anal_spin", "ring_synth", "ring_anal", "stage_alm",
             "scatter_alm", "mixed_image")
+LEGENDRE = FAMILIES[:6]
+# profile summary holding 'dram_bytes_per_launch: <int>' for each family
+TRAFFIC_FILE = {"mixed_anal_spin": "mixed_anal_spin2_nside2048.txt",
+                "mixed_anal_spin0": "mixed_anal_spin0_nside2048.txt",
+                "mixed_synth_spin": "mixed_synth_spin2_nside2048.txt",
+                "mixed_synth_spin0": "mixed_synth_spin0_nside2048.txt",
+                "legendre_anal": "legendre_anal_fp64_nside2048.txt",
+                "legendre_synth": "legendre_synth_fp64_nside2048.txt"}
 
 
 class Sets:
@@ -443,15 +454,15 @@ def main():
                     / np.linalg.norm(h_out[0][0]))
     rt_err = float(np.linalg.norm(h_out[0][0] - t_in) / np.linalg.norm(t_in))
 
-    # roofline of the dominant kernel family
-    dom = max(("legendre_synth", "legendre_anal"), key=lambda k: fam.get(k, (0, 0))[0])
+    # roofline of the dominant Legendre kernel family
+    dom = max((f for f in LEGENDRE if f in fam), key=lambda k: fam[k][0])
     dom_ms, dom_n = fam[dom]
-    roof = roofline(dom, dom_ms, dom_n, ops, B, mixed, args.steps, fp64_gemm_peak(torch))
+    roof = roofline(dom, dom_ms, dom_n, ops, B, args.steps, fp64_gemm_peak(torch))
     tot = sum(v[0] for v in fam.values())
     share = {k: round(v[0] / max(1e-9, tot), 4) for k, v in fam.items()}
 
     form = (f"mixed: batch of {B} sets per step, SHARP_MIXED (int8 tensor-core Legendre "
-            f"synthesis; analysis FP64)" if mixed else "fp64 drop-in, one set per step")
+            f"synthesis and analysis)" if mixed else "fp64 drop-in, one set per step")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -484,31 +495,35 @@ def main():
         dist.destroy_process_group()
 
 
-def roofline(dom, dom_ms, dom_n, ops, B, mixed, steps, peak):
+def roofline(dom, dom_ms, dom_n, ops, B, steps, peak):
     """Achieved FP64 rate of the dominant Legendre family against the
-    measured DGEMM peak.  FP64 kernels: the reference's operation count
-    (sharp_execute's opcnt).  Mixed synthesis: the FP64 work its producers
-    execute per (ring pair, l): recurrence plus quantisation, 5 flops at spin
-    0 and 12 at spin 2 (the contraction itself runs on the int8 tensor
-    pipe)."""
-    if dom == "legendre_synth":
-        if mixed:
-            v0 = ops["s0_synth"] / (4 + 4 * B)      # (ring pair, l) values of the spin-0 job
-            v2 = ops["s2_synth"] / (12 + 16 * B)
-            flops = 5 * v0 + 12 * v2
-            what = "mixed synthesis producer FP64 work (recurrence + quantisation)"
-        else:
-            flops = ops["s0_synth"] + ops["s2_synth"]
-            what = "reference operation count"
+    DGEMM peak measured in the same run, per launch.
+
+    FP64 kernels: the reference's operation count (sharp_execute's opcnt).
+    Mixed kernels: the FP64 work their producers execute per (ring pair, l)
+    value, the recurrence plus the quantisation of its values: 5 flops at
+    spin 0 (DMUL + 2 DFMA) and 12 at spin s (two recurrences of 2 DFMA each
+    plus two quantising DFMA); every launch covers all (ring pair, l) values
+    of its job.  The contraction itself runs on the int8 tensor pipe."""
+    job = {"legendre_synth": ("s0_synth", "s2_synth"), "legendre_anal": ("s0_anal", "s2_anal"),
+           "mixed_synth_spin0": ("s0_synth",), "mixed_synth_spin": ("s2_synth",),
+           "mixed_anal_spin0": ("s0_anal",), "mixed_anal_spin": ("s2_anal",)}[dom]
+    if dom.startswith("mixed"):
+        spin2 = dom.endswith("spin")
+        values = ops[job[0]] / ((12 + 16 * B) if spin2 else (4 + 4 * B))
+        flops_step = values * (12 if spin2 else 5) * dom_n / steps
+        what = "mixed-kernel producer FP64 work (recurrence + quantisation), all launches of a step"
     else:
-        flops = ops["s0_anal"] + ops["s2_anal"]
+        flops_step = sum(ops[j] for j in job)
         what = "reference operation count"
-    achieved = flops * steps / (dom_ms * 1e-3) / 1e12
+    achieved = flops_step * steps / (dom_ms * 1e-3) / 1e12
     return {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "work": what,
             "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-            "flops_per_step": flops, "ms_per_launch": dom_ms / max(dom_n, 1),
-            "traffic": dram_traffic_from_profiles()}
+            "flops_per_launch": flops_step * steps / max(dom_n, 1),
+            "ms_per_launch": dom_ms / max(dom_n, 1),
+            "launches_per_step": dom_n / steps,
+            "traffic": dram_traffic_from_profiles(dom)}
 
 
 if __name__ == "__main__":

@@ -582,7 +582,7 @@ void launch_shape(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp, co
     SHT_CUDA(cudaGetLastError());
   }
   {
-    ProfScope ps("legendre_synth", st);
+    ProfScope ps(S::T == 1 ? "mixed_synth_spin0" : "mixed_synth_spin", st);
     auto k = mixed_synth_kernel<S>;
     SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
     k<<<int(gp.mixed_items.size()), kThreads, S::SMEM, st>>>(

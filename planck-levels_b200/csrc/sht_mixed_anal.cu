@@ -529,7 +529,7 @@ template <class S>
 void launch_anal_shape(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp,
                        const double2 *phase, int ncm, int t0, double2 *Aout, int ncA,
                        int *d_err, cudaStream_t st) {
-  ProfScope ps("legendre_anal", st);
+  ProfScope ps(S::SPIN ? "mixed_anal_spin" : "mixed_anal_spin0", st);
   auto k = mixed_anal_kernel<S>;
   SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
   const int per = S::SPIN ? 2 : 1;   // maps and a_lm components per transform
