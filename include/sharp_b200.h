@@ -20,10 +20,14 @@ enum {
      Yt is the exact adjoint of Y under <a,b> = sum_{m=0} Re(a*b)
      + 2 sum_{m>0} Re(a*b) on a_lm and the plain dot product on maps. */
   SHARP_ADJOINT = 1<<8,
-  /* Mixed-precision execution: FP64 recurrence, tensor-core contraction of
-     the Legendre step on split TF32 operands with FP32 accumulation
-     (flushed to FP64 per l-block).  Results are within ~1e-6 relative L2 of
-     the FP64 path. */
+  /* Mixed-precision execution of alm2map and map2alm (any spin):
+     the recurrence stays FP64 on the CUDA cores; its values are quantised
+     to 32-bit fixed point against an analytic bound, the other operand to
+     signed base-256 digits, and the Legendre contraction runs exactly in
+     integers on the int8 tensor cores (int32 accumulation, combined in
+     64-bit integers and scaled to FP64 per l-tile).  Results are within
+     1e-6 relative L2 of the FP64 path (typically 1e-8).  Other job types
+     ignore the flag. */
   SHARP_MIXED   = 1<<9
 };
 
@@ -61,9 +65,39 @@ unsigned long long sharp_b200_kernel_launches (void);
 void sharp_b200_profile (int on);
 /* Waits for the recorded events and returns the summed milliseconds of all
    launches of one kernel family since profiling started ("legendre_synth",
-   "legendre_anal", "ring_synth", "ring_anal", "stage_alm", "scatter_alm");
-   *launches (if non-NULL) receives their number. */
+   "legendre_anal", "mixed_synth_spin0", "mixed_synth_spin",
+   "mixed_anal_spin0", "mixed_anal_spin", "mixed_image", "ring_synth",
+   "ring_anal", "stage_alm", "scatter_alm"); *launches (if non-NULL)
+   receives their number. */
 double sharp_b200_profile_ms (const char *family, unsigned long long *launches);
+
+/* One job of a batch: the arguments of sharp_execute. */
+typedef struct {
+  sharp_jobtype type;
+  int spin;
+  void *alm;                          /* ntrans * nalm pointers, as sharp_execute */
+  void *map;                          /* ntrans * nmaps pointers */
+  const sharp_geom_info *geom_info;
+  const sharp_alm_info *alm_info;
+  int ntrans;
+  int flags;
+} sharp_b200_job;
+
+/* Runs a batch of independent jobs of uneven geometry, lmax and spin (for
+   example many spin-0 and spin-2 maps at several HEALPix resolutions).
+   No counterpart in the reference, whose callers loop over sharp_execute.
+   Jobs that share type, spin, flags and the same geom_info and alm_info
+   objects are merged into one job of up to 100 transforms, so the batched
+   kernels (SHARP_MIXED) see them together; merged groups run in order of
+   first appearance on one stream.  Every output equals that of
+   sharp_execute on its own job (the merge changes no arithmetic).  Jobs
+   must not share output arrays.  device_ptrs = 0: host arrays, returns
+   after the results are copied back; 1: device arrays, work enqueued on
+   `stream` as sharp_b200_execute_device.  opcnt (if non-NULL) receives the
+   summed operation count.  Returns the number of merged groups executed,
+   or -1 after a failure in non-abort mode. */
+int sharp_b200_execute_batch (const sharp_b200_job *jobs, int njobs,
+  int device_ptrs, void *stream, unsigned long long *opcnt);
 
 /* Spin-0 alm2map without any device allocation.  No counterpart in the
    reference: it serves callers that cannot call cudaMalloc when they need a

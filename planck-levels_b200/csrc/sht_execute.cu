@@ -711,12 +711,70 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
   if (time) *time = wall_now() - t0;
 }
 
-void guarded(const std::function<void()> &fn) {
+bool guarded(const std::function<void()> &fn) {
   try {
     fn();
+    return true;
   } catch (const Failure &) {
     // message already recorded; non-aborting mode returns to the caller
+    return false;
   }
+}
+
+// Batch of independent jobs: jobs with the same type, spin, flags, geometry
+// and a_lm objects are merged (their pointer arrays concatenated in order) into
+// jobs of at most kMaxTrans transforms; each merged job runs through
+// execute_impl.  Returns the number of merged jobs.
+int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
+                       cudaStream_t stream, unsigned long long *opcnt) {
+  SHT_REQUIRE(njobs >= 0 && (jobs != nullptr || njobs == 0), "bad job list");
+  struct Group {
+    const sharp_b200_job *first;
+    std::vector<void *> alm, map;
+    int ntrans = 0;
+  };
+  std::vector<Group> groups;
+  // pointers per transform before the type remap (sharp.c:855-856)
+  auto counts = [](const sharp_b200_job &j, int &na, int &nm) {
+    const bool deriv = j.type == SHARP_ALM2MAP_DERIV1;
+    na = deriv ? 1 : (j.spin > 0 ? 2 : 1);
+    nm = (deriv || j.spin > 0) ? 2 : 1;
+  };
+  for (int i = 0; i < njobs; ++i) {
+    const sharp_b200_job &j = jobs[i];
+    SHT_REQUIRE(j.ntrans > 0 && j.ntrans <= kMaxTrans, "bad number of simultaneous transforms");
+    SHT_REQUIRE(j.alm != nullptr && j.map != nullptr, "null alm or map pointer array");
+    int na, nm;
+    counts(j, na, nm);
+    Group *g = nullptr;
+    for (auto &c : groups) {
+      const sharp_b200_job &f = *c.first;
+      if (f.type == j.type && f.spin == j.spin && f.flags == j.flags &&
+          f.geom_info == j.geom_info && f.alm_info == j.alm_info &&
+          c.ntrans + j.ntrans <= kMaxTrans) {
+        g = &c;
+        break;
+      }
+    }
+    if (!g) {
+      groups.push_back(Group{&j, {}, {}, 0});
+      g = &groups.back();
+    }
+    void *const *pa = static_cast<void *const *>(j.alm);
+    void *const *pm = static_cast<void *const *>(j.map);
+    g->alm.insert(g->alm.end(), pa, pa + size_t(j.ntrans) * na);
+    g->map.insert(g->map.end(), pm, pm + size_t(j.ntrans) * nm);
+    g->ntrans += j.ntrans;
+  }
+  unsigned long long tot = 0;
+  for (auto &g : groups) {
+    unsigned long long oc = 0;
+    execute_impl(g.first->type, g.first->spin, g.alm.data(), g.map.data(), g.first->geom_info,
+                 g.first->alm_info, g.ntrans, g.first->flags, device_ptrs, stream, nullptr, &oc);
+    tot += oc;
+  }
+  if (opcnt) *opcnt = tot;
+  return int(groups.size());
 }
 
 }  // namespace
@@ -756,6 +814,16 @@ void sharp_b200_execute_device(sharp_jobtype type, int spin, void *alm, void *ma
     sht::execute_impl(type, spin, alm, map, geom_info, alm_info, ntrans, flags, true,
                       static_cast<cudaStream_t>(stream), time, opcnt);
   });
+}
+
+int sharp_b200_execute_batch(const sharp_b200_job *jobs, int njobs, int device_ptrs,
+                             void *stream, unsigned long long *opcnt) {
+  int n = -1;
+  sht::guarded([&] {
+    n = sht::execute_batch_impl(jobs, njobs, device_ptrs != 0,
+                                static_cast<cudaStream_t>(stream), opcnt);
+  });
+  return n;
 }
 
 void sharp_b200_forget_geometry(const sharp_geom_info *info) {

@@ -128,10 +128,12 @@ class Geometry:
     def __init__(self, ptr):
         self.ptr = ptr
 
-    def __del__(self):
+    # the destructor is bound at class creation: module globals may already be
+    # cleared when objects are collected at interpreter exit
+    def __del__(self, _destroy=_lib.sharp_destroy_geom_info):
         p = getattr(self, "ptr", None)
         if p:
-            _lib.sharp_destroy_geom_info(p)
+            _destroy(p)
             self.ptr = None
 
     @property
@@ -188,10 +190,10 @@ class AlmInfo:
     def __init__(self, ptr):
         self.ptr = ptr
 
-    def __del__(self):
+    def __del__(self, _destroy=_lib.sharp_destroy_alm_info):
         p = getattr(self, "ptr", None)
         if p:
-            _lib.sharp_destroy_alm_info(p)
+            _destroy(p)
             self.ptr = None
 
     @property
@@ -280,3 +282,39 @@ def execute_device(jtype: int, spin: int, alm, maps, geom: Geometry, ainfo: AlmI
                                    C.c_void_p(stream.cuda_stream), None, C.byref(op))
     _check()
     return op.value
+
+
+class sharp_b200_job(C.Structure):
+    _fields_ = [("type", C.c_int), ("spin", C.c_int), ("alm", C.c_void_p), ("map", C.c_void_p),
+                ("geom_info", C.POINTER(sharp_geom_info)),
+                ("alm_info", C.POINTER(sharp_alm_info)), ("ntrans", C.c_int), ("flags", C.c_int)]
+
+
+_lib.sharp_b200_execute_batch.argtypes = [C.POINTER(sharp_b200_job), C.c_int, C.c_int,
+                                          C.c_void_p, C.POINTER(C.c_ulonglong)]
+_lib.sharp_b200_execute_batch.restype = C.c_int
+
+
+def execute_batch(jobs, device: bool = False, stream=None):
+    """sharp_b200_execute_batch: ``jobs`` is a list of tuples
+    (jtype, spin, alm, maps, geom, ainfo, ntrans, flags) with alm/maps lists
+    of numpy arrays (device=False) or CUDA tensors (device=True), as in
+    ``execute`` / ``execute_device``.  Compatible jobs are merged into one
+    batched job.  Returns (number of merged jobs, operation count)."""
+    keep = []
+    arr = (sharp_b200_job * max(len(jobs), 1))()
+    for i, (jt, spin, alm, maps, geom, ainfo, nt, fl) in enumerate(jobs):
+        ptr = (lambda a: a.data_ptr()) if device else (lambda a: a.ctypes.data)
+        aptr = (C.c_void_p * len(alm))(*[ptr(a) for a in alm])
+        mptr = (C.c_void_p * len(maps))(*[ptr(m) for m in maps])
+        keep += [aptr, mptr]
+        arr[i] = sharp_b200_job(jt, spin, C.cast(aptr, C.c_void_p), C.cast(mptr, C.c_void_p),
+                                geom.ptr, ainfo.ptr, nt, fl)
+    st = None
+    if device:
+        import torch
+        st = C.c_void_p((stream or torch.cuda.current_stream()).cuda_stream)
+    op = C.c_ulonglong(0)
+    n = _lib.sharp_b200_execute_batch(arr, len(jobs), 1 if device else 0, st, C.byref(op))
+    _check()
+    return n, op.value

@@ -153,6 +153,24 @@ def test_bad_arguments_report_errors_without_abort():
         sb.set_abort_on_error(os.environ.get("SHARP_B200_ABORT_ON_ERROR", "1") != "0")
 
 
+def test_batch_validates_jobs_before_running():
+    # every job is checked before the first one runs: a bad job anywhere in
+    # the list fails the call with the single-job message
+    sb.set_abort_on_error(False)
+    try:
+        g = sb.Geometry.healpix(4)
+        a = sb.AlmInfo.triangular(8)
+        alm = [np.zeros(sb.nalm_triangular(8), np.complex128)]
+        mp = [np.zeros(192)]
+        good = (sb.SHARP_ALM2MAP, 0, alm, mp, g, a, 1, sb.SHARP_DP)
+        bad = (sb.SHARP_ALM2MAP, 0, alm, mp, g, a, 0, sb.SHARP_DP)
+        with pytest.raises(sb.SharpError, match="bad number of simultaneous transforms"):
+            sb.execute_batch([good, bad])
+        assert sb.execute_batch([]) == (0, 0)
+    finally:
+        sb.set_abort_on_error(os.environ.get("SHARP_B200_ABORT_ON_ERROR", "1") != "0")
+
+
 def test_bad_arguments_abort_like_reference_by_default():
     code = (
         "import sys; sys.path.insert(0, %r)\n"

@@ -1,0 +1,157 @@
+"""sharp_b200_execute_batch: a batch of independent jobs of uneven HEALPix
+resolution, lmax and spin (the shape of the batched configuration: spin-0
+and spin-2 TEB -> IQU sets with Nside drawn from a small set and
+lmax = 2 Nside, E/B spectra 0.1 and 0.01 of T), at sizes the tests finish in
+seconds.  Each output must equal sharp_execute on its own job (FP64), and the
+SHARP_MIXED batch must stay within 1e-6 relative L2 of FP64 per map."""
+import numpy as np
+import pytest
+
+import sharp_b200 as sb
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+DP, MIXED = sb.SHARP_DP, sb.SHARP_MIXED
+TOL_MIXED = 1e-6
+
+
+def _cl(lmax, fwhm_arcmin=5.0):
+    l = np.arange(lmax + 1, dtype=np.float64)
+    sig = fwhm_arcmin * np.pi / 10800.0
+    cl = np.exp(-l * (l + 1) * sig * sig) / (l + 1) ** 2
+    cl[:2] = 0.0
+    return cl
+
+
+def _alm(lmax, cl, rng):
+    out = np.zeros(sb.nalm_triangular(lmax), np.complex128)
+    i = 0
+    for m in range(lmax + 1):
+        n = lmax + 1 - m
+        a = np.sqrt(cl[m:])
+        if m == 0:
+            out[i:i + n] = a * rng.standard_normal(n)
+        else:
+            out[i:i + n] = a * np.sqrt(0.5) * (rng.standard_normal(n)
+                                               + 1j * rng.standard_normal(n))
+        i += n
+    return out
+
+
+def _mix(nsides=(16, 32, 64), n0=12, n2=4, seed=0):
+    """Uneven mix: n0 spin-0 (T) and n2 spin-2 (E, B) sets, Nside uniform over
+    nsides, lmax = 2 Nside; one geometry / a_lm object per resolution."""
+    rng = np.random.default_rng(seed)
+    geo = {n: (sb.Geometry.healpix(n), sb.AlmInfo.triangular(2 * n)) for n in nsides}
+    sets = []
+    for k in range(n0 + n2):
+        spin = 0 if k < n0 else 2
+        n = int(rng.choice(nsides))
+        cl = _cl(2 * n)
+        alms = [_alm(2 * n, cl, rng)] if spin == 0 else \
+            [_alm(2 * n, 0.1 * cl, rng), _alm(2 * n, 0.01 * cl, rng)]
+        sets.append((spin, n, alms))
+    order = rng.permutation(len(sets))   # interleave spins and resolutions
+    return geo, [sets[i] for i in order]
+
+
+def _run_batch(geo, sets, jtype, flags, inputs):
+    """One batch call; inputs[i] are the set's input arrays (alm for alm2map,
+    maps for map2alm).  Returns the outputs."""
+    jobs, outs = [], []
+    for (spin, n, _), inp in zip(sets, inputs):
+        g, a = geo[n]
+        if jtype == sb.SHARP_ALM2MAP:
+            out = [np.zeros(12 * n * n) for _ in inp]
+            jobs.append((jtype, spin, [x.copy() for x in inp], out, g, a, 1, flags))
+        else:
+            out = [np.zeros(sb.nalm_triangular(2 * n), np.complex128) for _ in inp]
+            jobs.append((jtype, spin, out, [x.copy() for x in inp], g, a, 1, flags))
+        outs.append(out)
+    ngroups, _ = sb.execute_batch(jobs)
+    return ngroups, outs
+
+
+def _run_single(geo, sets, jtype, flags, inputs):
+    outs = []
+    for (spin, n, _), inp in zip(sets, inputs):
+        g, a = geo[n]
+        if jtype == sb.SHARP_ALM2MAP:
+            out = [np.zeros(12 * n * n) for _ in inp]
+            sb.execute(jtype, spin, [x.copy() for x in inp], out, g, a, 1, flags)
+        else:
+            out = [np.zeros(sb.nalm_triangular(2 * n), np.complex128) for _ in inp]
+            sb.execute(jtype, spin, out, [x.copy() for x in inp], g, a, 1, flags)
+        outs.append(out)
+    return outs
+
+
+def test_batch_matches_single_jobs_fp64():
+    geo, sets = _mix()
+    alms = [s[2] for s in sets]
+    ng, maps_b = _run_batch(geo, sets, sb.SHARP_ALM2MAP, DP, alms)
+    assert ng == len({(s[0], s[1]) for s in sets})   # one merged job per (spin, Nside)
+    maps_s = _run_single(geo, sets, sb.SHARP_ALM2MAP, DP, alms)
+    for xb, xs in zip(maps_b, maps_s):
+        for x, y in zip(xb, xs):
+            assert rel_l2(x, y) < 1e-13
+    _, alm_b = _run_batch(geo, sets, sb.SHARP_MAP2ALM, DP, maps_s)
+    alm_s = _run_single(geo, sets, sb.SHARP_MAP2ALM, DP, maps_s)
+    for xb, xs in zip(alm_b, alm_s):
+        for x, y in zip(xb, xs):
+            assert rel_l2(x, y) < 1e-13
+
+
+def test_batch_mixed_error_per_map():
+    geo, sets = _mix(seed=1)
+    alms = [s[2] for s in sets]
+    _, m64 = _run_batch(geo, sets, sb.SHARP_ALM2MAP, DP, alms)
+    _, mmx = _run_batch(geo, sets, sb.SHARP_ALM2MAP, DP | MIXED, alms)
+    for xb, xs in zip(mmx, m64):
+        for x, y in zip(xb, xs):
+            assert rel_l2(x, y) < TOL_MIXED
+    _, a64 = _run_batch(geo, sets, sb.SHARP_MAP2ALM, DP, m64)
+    _, amx = _run_batch(geo, sets, sb.SHARP_MAP2ALM, DP | MIXED, m64)
+    for xb, xs in zip(amx, a64):
+        for x, y in zip(xb, xs):
+            assert rel_l2(x, y) < TOL_MIXED
+
+
+def test_batch_against_reference():
+    import ref
+    if not ref.available():
+        pytest.skip("reference library not built (make -C oracle)")
+    geo, sets = _mix(nsides=(16, 32), n0=3, n2=2, seed=2)
+    alms = [s[2] for s in sets]
+    _, maps_b = _run_batch(geo, sets, sb.SHARP_ALM2MAP, DP, alms)
+    rgeo = {n: (ref.healpix(n), ref.triangular(2 * n, 2 * n)) for n in (16, 32)}
+    for (spin, n, _), inp, got in zip(sets, alms, maps_b):
+        g, a = rgeo[n]
+        out = [np.zeros(12 * n * n) for _ in inp]
+        ref.execute(sb.SHARP_ALM2MAP, spin, [x.copy() for x in inp], out, g, a, 1, DP)
+        for x, y in zip(got, out):
+            assert rel_l2(x, y) < 1e-12
+
+
+def test_batch_device_pointers_and_merge_limit():
+    import torch
+    dev = torch.device("cuda:0")
+    nside, lmax = 16, 32
+    g, a = sb.Geometry.healpix(nside), sb.AlmInfo.triangular(lmax)
+    rng = np.random.default_rng(3)
+    nalm = sb.nalm_triangular(lmax)
+    # 60 + 60 single-transform jobs: merged into two jobs (at most 100 each)
+    alms = [rng.standard_normal(nalm) + 1j * rng.standard_normal(nalm) for _ in range(120)]
+    for x in alms:
+        x[:lmax + 1] = x[:lmax + 1].real
+    ta = [torch.view_as_real(torch.from_numpy(x).to(dev)).reshape(-1) for x in alms]
+    tm = [torch.zeros(12 * nside * nside, dtype=torch.float64, device=dev) for _ in alms]
+    jobs = [(sb.SHARP_ALM2MAP, 0, [ta[i]], [tm[i]], g, a, 1, DP) for i in range(120)]
+    ng, op = sb.execute_batch(jobs, device=True)
+    torch.cuda.synchronize()
+    assert ng == 2 and op > 0
+    for i in (0, 57, 119):
+        ref_map = [np.zeros(12 * nside * nside)]
+        sb.execute(sb.SHARP_ALM2MAP, 0, [alms[i].copy()], ref_map, g, a, 1, DP)
+        assert rel_l2(tm[i].cpu().numpy(), ref_map[0]) < 1e-13
+
