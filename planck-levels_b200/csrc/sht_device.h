@@ -146,6 +146,16 @@ void launch_bluestein_setup_preplaced(const GeomPlan &gp, const int *d_blue_idx,
 // map_lo / alm_lo: index (in elements of the user array) that the device
 // pointers in maps_dev / alm_dev point at (0 when they are the user's own
 // device arrays, the extent start when they are staged copies).
+// Ring FFT shared memory.  Entries of the high twiddle slice for ring lengths
+// up to 2 nmax_complex, and the double2 entries of one CTA: buffers A and B,
+// the phi0 shift slices (64 + mmax/64 + 2), the twiddle slices of the ring
+// length and of the Bluestein convolution length P (64 + P/64 + 2).
+inline int ring_twiddle_hi_entries(int nmax_complex) { return (2 * nmax_complex) / 64 + 2; }
+inline size_t ring_fft_smem_entries(int bufA, int bufB, int mmax, int nmax_complex, int P) {
+  return size_t(bufA) + bufB + (64 + mmax / 64 + 2) + (64 + ring_twiddle_hi_entries(nmax_complex)) +
+         (64 + P / 64 + 2);
+}
+
 void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                        const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
                        cudaStream_t st);

@@ -245,10 +245,7 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
       gp->cls_start.push_back(int(flat.size()));
       gp->cls_count.push_back(int(lists[c].size()));
       flat.insert(flat.end(), lists[c].begin(), lists[c].end());
-      const size_t smem = sizeof(double2) * (bufA + bufB + 64 + mmax / 64 + 2);
-      SHT_REQUIRE(smem <= 227 * 1024,
-                  "ring length exceeds the shared-memory FFT limit (about 8000 pixels for "
-                  "lengths with large prime factors, 13900 otherwise)");
+      // classes whose buffers exceed shared memory run them in global scratch
     }
     gp->cls_pairs = dev_upload(flat, st);
   }

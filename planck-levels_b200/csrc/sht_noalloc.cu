@@ -179,6 +179,8 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
     lists[c].push_back(p);
   }
   std::vector<int> flat, cls_N, cls_start, cls_count, cls_bufA, cls_bufB;
+  int nmax_all = 1;
+  for (const FftDesc &d : descs) nmax_all = std::max(nmax_all, d.N);
   for (int c = 0; c < 4; ++c) {
     int bufA = 2, bufB = 2, nmaxc = 1;
     for (int p : lists[c])
@@ -195,7 +197,8 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
     cls_start.push_back(int(flat.size()));
     cls_count.push_back(int(lists[c].size()));
     flat.insert(flat.end(), lists[c].begin(), lists[c].end());
-    SHT_REQUIRE(sizeof(double2) * (bufA + bufB + 64 + mmax / 64 + 2) <= 227 * 1024,
+    SHT_REQUIRE(sizeof(double2) * ring_fft_smem_entries(bufA, bufB, mmax, nmax_all, P) <=
+                    227 * 1024,
                 "ring length exceeds the shared-memory FFT limit");
   }
   // recurrence tables
@@ -290,6 +293,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
     }
   } release{gp, cp, ap};
   gp.lmax = lmax; gp.mmax = mmax; gp.spin = 0; gp.npairs = np; gp.nphmax = g->nphmax;
+  gp.nmax_complex = nmax_all;
   gp.count_m = count; gp.synth_items = items; gp.synth_tile = tile;
   gp.cth = static_cast<double *>(at(o_cth)); gp.sth = static_cast<double *>(at(o_sth));
   gp.mlim = static_cast<int *>(at(o_mlim)); gp.count = static_cast<int *>(at(o_count));

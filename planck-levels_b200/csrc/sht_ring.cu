@@ -13,9 +13,13 @@
 // odd lengths a complex FFT of length n.  Radix-2/3/4/5 stages and a generic
 // prime stage share one code path (each thread computes whole outputs, so
 // large prime factors parallelise over outputs).  Twiddles come from a
-// per-length table exp(-2 pi i j/n) computed once per geometry.
+// per-length table exp(-2 pi i j/n) computed once per geometry; each ring
+// copies two short slices of it into shared memory (e mod 64 and 64 (e/64))
+// and forms exp(-2 pi i e/n) as their product, so no butterfly waits on a
+// global load.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "sht_device.h"
@@ -39,6 +43,28 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) {
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) {
   return make_double2(a.x * s, a.y * s);
+}
+
+// exp(-2 pi i e/n), 0 <= e < n, read from the per-length global table
+struct TwGlobal {
+  const double2 *__restrict__ W;
+  __device__ __forceinline__ double2 operator()(int e) const { return __ldg(W + e); }
+};
+// the same from two shared-memory slices: lo[e mod 64] * hi[e / 64]
+constexpr int kTwLo = 64;
+struct TwShared {
+  const double2 *lo, *hi;
+  __device__ __forceinline__ double2 operator()(int e) const {
+    return cmul(hi[e >> 6], lo[e & (kTwLo - 1)]);
+  }
+};
+// Copies the slices of the table W (n entries) into lo (64) and hi (n/64 + 1).
+__device__ void load_twshared(double2 *lo, double2 *hi, const double2 *__restrict__ W, int n) {
+  const int nhi = (n + kTwLo - 1) / kTwLo;
+  for (int t = threadIdx.x; t < kTwLo + nhi; t += blockDim.x) {
+    if (t < kTwLo) lo[t] = t < n ? __ldg(W + t) : make_double2(1.0, 0.0);
+    else hi[t - kTwLo] = __ldg(W + kTwLo * (t - kTwLo));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -93,9 +119,9 @@ __device__ __forceinline__ void small_dft(double2 (&v)[R], bool inv) {
   }
 }
 
-template <int R>
+template <int R, class TW>
 __device__ void stockham_small(const double2 *src, double2 *dst, int N, int Ns, bool inv,
-                               const double2 *__restrict__ W, int step) {
+                               const TW &tw, int step) {
   const int NR = N / R;
   const int sf = N / (Ns * R);
   for (int j = threadIdx.x; j < NR; j += blockDim.x) {
@@ -106,7 +132,7 @@ __device__ void stockham_small(const double2 *src, double2 *dst, int N, int Ns, 
     if (Ns > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        double2 w = __ldg(W + (long long)r * k * sf * step);
+        double2 w = tw(r * k * sf * step);
         if (inv) w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
@@ -120,8 +146,9 @@ __device__ void stockham_small(const double2 *src, double2 *dst, int N, int Ns, 
 
 // Generic prime radix: each thread computes whole outputs (parallel over
 // the N outputs, so a large prime factor does not serialise a few threads).
+template <class TW>
 __device__ void stockham_generic(const double2 *src, double2 *dst, int N, int R, int Ns,
-                                 bool inv, const double2 *__restrict__ W, int step) {
+                                 bool inv, const TW &tw, int step) {
   const int NR = N / R;
   const int sf = N / (Ns * R);
   for (int item = threadIdx.x; item < N; item += blockDim.x) {
@@ -132,7 +159,7 @@ __device__ void stockham_generic(const double2 *src, double2 *dst, int N, int R,
     int e = 0;
     double2 acc = make_double2(0.0, 0.0);
     for (int r = 0; r < R; ++r) {
-      double2 w = __ldg(W + (long long)e * step);
+      double2 w = tw(e * step);
       if (inv) w.y = -w.y;
       const double2 v = src[j + r * NR];
       acc.x = fma(v.x, w.x, fma(-v.y, w.y, acc.x));
@@ -147,9 +174,8 @@ __device__ void stockham_generic(const double2 *src, double2 *dst, int N, int R,
 // Complex FFT of length d.N in buffers a/b; returns the buffer holding the
 // result.  Callers synchronise before; the function synchronises after each
 // pass.
-__device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv,
-                            const double2 *__restrict__ twiddle) {
-  const double2 *W = twiddle + d.tw;
+template <class TW>
+__device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv, const TW &W) {
   const int step = d.n / d.N;
   int Ns = 1;
   double2 *src = a, *dst = b;
@@ -179,14 +205,16 @@ __device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv,
 // transform precomputed in the same order, decimation-in-time back to
 // natural order.  The inverse transform is conj(forward(conj x)).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double2 chirp_of(int j, int n, int N, const double2 *__restrict__ Wn) {
-  if ((n & 1) == 0) return __ldg(Wn + (int)(((long long)j * j) % n));  // exp(-2 pi i (j^2 mod n)/n)
+template <class TW>
+__device__ __forceinline__ double2 chirp_of(int j, int n, int N, const TW &Wn) {
+  if ((n & 1) == 0) return Wn(int(((long long)j * j) % n));  // exp(-2 pi i (j^2 mod n)/n)
   double sn, cs;
   sincospi(-double(((long long)j * j) % (2ll * n)) / n, &sn, &cs);
   return make_double2(cs, sn);
 }
 
-__device__ void dif_inplace(double2 *a, int M, const double2 *__restrict__ Wp, int P) {
+template <class TW>
+__device__ void dif_inplace(double2 *a, int M, const TW &Wp, int P) {
   int lg = 31 - __clz(M);
   for (int len = M; len >= 2; len >>= 1, --lg) {
     const int half = len >> 1, st = P / len;
@@ -195,20 +223,21 @@ __device__ void dif_inplace(double2 *a, int M, const double2 *__restrict__ Wp, i
       const int b0 = blk * len + i;
       const double2 u = a[b0], v = a[b0 + half];
       a[b0] = cadd(u, v);
-      a[b0 + half] = cmul(csub(u, v), __ldg(Wp + i * st));
+      a[b0 + half] = cmul(csub(u, v), Wp(i * st));
     }
     __syncthreads();
   }
 }
 
-__device__ void dit_inplace_inv(double2 *a, int M, const double2 *__restrict__ Wp, int P) {
+template <class TW>
+__device__ void dit_inplace_inv(double2 *a, int M, const TW &Wp, int P) {
   int lg = 1;
   for (int len = 2; len <= M; len <<= 1, ++lg) {
     const int half = len >> 1, st = P / len;
     for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
       const int blk = t >> (lg - 1), i = t & (half - 1);
       const int b0 = blk * len + i;
-      const double2 u = a[b0], v = cmul(a[b0 + half], cconj(__ldg(Wp + i * st)));
+      const double2 u = a[b0], v = cmul(a[b0 + half], cconj(Wp(i * st)));
       a[b0] = cadd(u, v);
       a[b0 + half] = csub(u, v);
     }
@@ -217,11 +246,9 @@ __device__ void dit_inplace_inv(double2 *a, int M, const double2 *__restrict__ W
 }
 
 // Input x in buf[0, N); buf holds M entries.  Result in buf[0, N).
-__device__ void run_bluestein(const FftDesc &d, double2 *buf, bool inv,
-                              const double2 *__restrict__ twiddle,
-                              const double2 *__restrict__ wpow2, int P,
-                              const double2 *__restrict__ bhat) {
-  const double2 *Wn = twiddle + d.tw;
+template <class TW>
+__device__ void run_bluestein(const FftDesc &d, double2 *buf, bool inv, const TW &Wn,
+                              const TW &wpow2, int P, const double2 *__restrict__ bhat) {
   const double2 *bh = bhat + d.bhat;
   for (int j = threadIdx.x; j < d.M; j += blockDim.x) {
     if (j < d.N) {
@@ -254,7 +281,7 @@ __global__ void bluestein_setup_kernel(const FftDesc *__restrict__ fdesc,
                                        double2 *__restrict__ bhat) {
   const FftDesc d = fdesc[blue_idx[blockIdx.x]];
   double2 *b = bhat + d.bhat;
-  const double2 *Wn = twiddle + d.tw;
+  const TwGlobal Wn{twiddle + d.tw};
   for (int j = threadIdx.x; j < d.M; j += blockDim.x) {
     int jj = -1;
     if (j < d.N) jj = j;
@@ -262,7 +289,7 @@ __global__ void bluestein_setup_kernel(const FftDesc *__restrict__ fdesc,
     b[j] = (jj >= 0) ? cconj(chirp_of(jj, d.n, d.N, Wn)) : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  dif_inplace(b, d.M, wpow2, P);
+  dif_inplace(b, d.M, TwGlobal{wpow2}, P);
   const double inv_m = 1.0 / d.M;
   for (int j = threadIdx.x; j < d.M; j += blockDim.x) b[j] = cscale(b[j], inv_m);
 }
@@ -307,19 +334,32 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
                                   const double2 *__restrict__ wpow2, int P,
                                   const double2 *__restrict__ bhat,
                                   const double2 *__restrict__ phase, int ncm, int mmax, int flags,
-                                  int nbufA, int nbufB, T *const *__restrict__ maps,
-                                  long long map_lo) {
+                                  int nbufA, int nbufB, int twcap, T *const *__restrict__ maps,
+                                  long long map_lo, double2 *__restrict__ gbuf, int npc,
+                                  int nitems) {
   extern __shared__ double2 smem[];
-  const int p = pairs[blockIdx.x];
-  const int c = blockIdx.y;
   const int ms = mmax + 1;
-  const int mm = min(mmax, mlim[p]);
   const bool add = (flags & SHARP_ADD) != 0;
   const double wscale = (flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0;
-  double2 *bufA = smem;
-  double2 *bufB = smem + nbufA;
-  double2 *slo = smem + nbufA + nbufB;
+  // buffers A/B in shared memory, or (rings too long for it) in this CTA's
+  // slot of a global scratch; such CTAs loop over (pair, component) items
+  const bool gb = gbuf != nullptr;
+  double2 *bufA = gb ? gbuf + size_t(blockIdx.x) * (nbufA + nbufB) : smem;
+  double2 *bufB = bufA + nbufA;
+  double2 *slo = gb ? smem : smem + nbufA + nbufB;
   double2 *shi = slo + kShiftLo;
+  // twiddle slices: ring length (twcap = 2 nmax/64 + 2 entries in hi), then
+  // the Bluestein convolution length P
+  double2 *twlo = shi + (mmax / kShiftLo + 2);
+  double2 *twhi = twlo + kTwLo;
+  double2 *pwlo = twhi + twcap;
+  double2 *pwhi = pwlo + kTwLo;
+  const TwShared tw{twlo, twhi}, pw{pwlo, pwhi};
+  if (P > 0) load_twshared(pwlo, pwhi, wpow2, P);
+  for (int it = gb ? blockIdx.x : 0; it < (gb ? nitems : 1); it += gb ? gridDim.x : 1) {
+  const int p = gb ? pairs[it % npc] : pairs[blockIdx.x];
+  const int c = gb ? it / npc : blockIdx.y;
+  const int mm = min(mmax, mlim[p]);
   T *map = maps[c];
   for (int h = 0; h < 2; ++h) {
     const int ring = 2 * p + h;
@@ -332,10 +372,9 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
     const int half = n / 2;  // highest bin kept (n odd: (n-1)/2)
     double2 *C = bufB;
     const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
-    if (rot) {
-      build_shift(slo, shi, mm, ph);
-      __syncthreads();
-    }
+    if (rot) build_shift(slo, shi, mm, ph);
+    load_twshared(twlo, twhi, twiddle + d.tw, n);
+    __syncthreads();
     // fold phase_m * wgt * e^{i m phi0} into bins 0..half (sharp.c:265-300)
     for (int k = threadIdx.x; k <= half; k += blockDim.x) {
       double2 acc = make_double2(0.0, 0.0);
@@ -353,13 +392,12 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
       C[k] = acc;
     }
     __syncthreads();
-    const double2 *W = twiddle + d.tw;
     if ((n & 1) == 0) {
       // Z_k = (C_k + conj C_{N-k}) + i conj(W^k) (C_k - conj C_{N-k}), k < N
       for (int k = threadIdx.x; k < d.N; k += blockDim.x) {
         const double2 ck = C[k], cn = cconj(C[d.N - k]);
         const double2 sm = cadd(ck, cn), df = csub(ck, cn);
-        const double2 w = __ldg(W + k);             // exp(-2 pi i k/n)
+        const double2 w = tw(k);                    // exp(-2 pi i k/n)
         const double2 iw = make_double2(w.y, w.x);  // i * conj(w)
         bufA[k] = cadd(sm, cmul(iw, df));
       }
@@ -370,10 +408,10 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
     __syncthreads();
     double2 *res;
     if (d.blue) {
-      run_bluestein(d, bufA, true, twiddle, wpow2, P, bhat);
+      run_bluestein(d, bufA, true, tw, pw, P, bhat);
       res = bufA;
     } else {
-      res = run_fft(d, bufA, bufB, true, twiddle);
+      res = run_fft(d, bufA, bufB, true, tw);
     }
     const long long o = ofs[ring] - map_lo;
     const long long st = stride[ring];
@@ -387,6 +425,7 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
       for (int j = threadIdx.x; j < n; j += blockDim.x) store_px(map + o + j * st, res[j].x, add);
     }
     __syncthreads();
+  }
   }
 }
 
@@ -402,18 +441,29 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
                                   const double2 *__restrict__ twiddle,
                                   const double2 *__restrict__ wpow2, int P,
                                   const double2 *__restrict__ bhat, double2 *__restrict__ phase,
-                                  int ncm, int mmax, int flags, int nbufA, int nbufB,
-                                  const T *const *__restrict__ maps, long long map_lo) {
+                                  int ncm, int mmax, int flags, int nbufA, int nbufB, int twcap,
+                                  const T *const *__restrict__ maps, long long map_lo,
+                                  double2 *__restrict__ gbuf, int npc, int nitems) {
   extern __shared__ double2 smem[];
-  const int p = pairs[blockIdx.x];
-  const int c = blockIdx.y;
   const int ms = mmax + 1;
-  const int mm = min(mmax, mlim[p]);
   const double wscale = (flags & SHARP_REAL_HARMONICS) ? kSqrtTwo : 1.0;
-  double2 *bufA = smem;
-  double2 *bufB = smem + nbufA;
-  double2 *slo = smem + nbufA + nbufB;
+  const bool gb = gbuf != nullptr;  // as in phase2ring_kernel
+  double2 *bufA = gb ? gbuf + size_t(blockIdx.x) * (nbufA + nbufB) : smem;
+  double2 *bufB = bufA + nbufA;
+  double2 *slo = gb ? smem : smem + nbufA + nbufB;
   double2 *shi = slo + kShiftLo;
+  // twiddle slices: ring length (twcap = 2 nmax/64 + 2 entries in hi), then
+  // the Bluestein convolution length P
+  double2 *twlo = shi + (mmax / kShiftLo + 2);
+  double2 *twhi = twlo + kTwLo;
+  double2 *pwlo = twhi + twcap;
+  double2 *pwhi = pwlo + kTwLo;
+  const TwShared tw{twlo, twhi}, pw{pwlo, pwhi};
+  if (P > 0) load_twshared(pwlo, pwhi, wpow2, P);
+  for (int it = gb ? blockIdx.x : 0; it < (gb ? nitems : 1); it += gb ? gridDim.x : 1) {
+  const int p = gb ? pairs[it % npc] : pairs[blockIdx.x];
+  const int c = gb ? it / npc : blockIdx.y;
+  const int mm = min(mmax, mlim[p]);
   const T *map = maps[c];
   for (int h = 0; h < 2; ++h) {
     const int ring = 2 * p + h;
@@ -426,6 +476,7 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
     const long long o = ofs[ring] - map_lo;
     const long long st = stride[ring];
     if (rot) build_shift(slo, shi, mm, -ph);
+    load_twshared(twlo, twhi, twiddle + d.tw, n);
     if ((n & 1) == 0) {
       for (int j = threadIdx.x; j < d.N; j += blockDim.x)
         bufA[j] = make_double2(double(map[o + (2 * j) * st]), double(map[o + (2 * j + 1) * st]));
@@ -436,20 +487,19 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
     __syncthreads();
     double2 *res;
     if (d.blue) {
-      run_bluestein(d, bufA, false, twiddle, wpow2, P, bhat);
+      run_bluestein(d, bufA, false, tw, pw, P, bhat);
       res = bufA;
     } else {
-      res = run_fft(d, bufA, bufB, false, twiddle);
+      res = run_fft(d, bufA, bufB, false, tw);
     }
     double2 *X = (res == bufA) ? bufB : bufA;
-    const double2 *W = twiddle + d.tw;
     if ((n & 1) == 0) {
       // X_k = (Z_k + conj Z_{N-k})/2 - i W^k (Z_k - conj Z_{N-k})/2, k <= N
       for (int k = threadIdx.x; k <= d.N; k += blockDim.x) {
         const double2 zk = res[k == d.N ? 0 : k];
         const double2 zn = cconj(res[k == 0 ? 0 : d.N - k]);
         const double2 sm = cadd(zk, zn), df = csub(zk, zn);
-        const double2 w = __ldg(W + k);
+        const double2 w = tw(k);
         const double2 mi_w = make_double2(w.y, -w.x);  // -i * w
         double2 xk = cscale(cadd(sm, cmul(mi_w, df)), 0.5);
         if (k == 0 || k == d.N) xk.y = 0.0;  // DC and Nyquist are real
@@ -472,6 +522,7 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
       dst[m] = v;
     }
     __syncthreads();
+  }
   }
 }
 
@@ -696,9 +747,81 @@ void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cud
 }
 
 static size_t fft_smem(const GeomPlan &gp, int cls, int mmax) {
-  return sizeof(double2) * (gp.cls_bufA[cls] + gp.cls_bufB[cls] + 64 + mmax / 64 + 2);
+  return sizeof(double2) * ring_fft_smem_entries(gp.cls_bufA[cls], gp.cls_bufB[cls], mmax,
+                                                 gp.nmax_complex, gp.P);
 }
+static int fft_twcap(const GeomPlan &gp) { return ring_twiddle_hi_entries(gp.nmax_complex); }
 static int fft_threads(int N) { return N <= 256 ? 64 : N <= 1024 ? 256 : 1024; }
+
+namespace {
+
+// Launch shape of one size class.  A class whose buffers exceed the shared
+// memory of a CTA keeps only the phi0 and twiddle slices there and runs its
+// buffers in a global scratch of two slots per SM (persistent CTAs).
+constexpr size_t kSmemLimit = 227 * 1024;
+struct FftLaunch {
+  dim3 grid;
+  int thr = 0;
+  size_t smem = 0;
+  double2 *gbuf = nullptr;
+  int npc = 0, nitems = 0;
+};
+FftLaunch plan_fft_launch(const GeomPlan &gp, int cls, int mmax, int ncomp, cudaStream_t st) {
+  FftLaunch L;
+  L.npc = gp.cls_count[cls];
+  L.nitems = L.npc * ncomp;
+  L.thr = fft_threads(gp.cls_N[cls]);
+  L.smem = fft_smem(gp, cls, mmax);
+  L.grid = dim3(L.npc, ncomp);
+  if (L.smem > kSmemLimit) {
+    int dev = 0, nsm = 0;
+    SHT_CUDA(cudaGetDevice(&dev));
+    SHT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int slots = std::min(L.nitems, 2 * std::max(nsm, 1));
+    L.grid = dim3(slots, 1);
+    L.thr = 1024;
+    L.smem = sizeof(double2) * ring_fft_smem_entries(0, 0, mmax, gp.nmax_complex, gp.P);
+    SHT_CUDA(cudaMallocAsync(&L.gbuf, sizeof(double2) * size_t(slots) *
+                                          (gp.cls_bufA[cls] + gp.cls_bufB[cls]), st));
+  }
+  return L;
+}
+
+template <typename T>
+void phase2ring_class(const JobDesc &job, const GeomPlan &gp, int cls, long long map_lo,
+                      const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                      cudaStream_t st) {
+  const FftLaunch L = plan_fft_launch(gp, cls, job.mmax, nmapptr, st);
+  auto k = phase2ring_kernel<T>;
+  SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L.smem)));
+  k<<<L.grid, L.thr, L.smem, st>>>(gp.cls_pairs + gp.cls_start[cls], gp.mlim, gp.nph, gp.ofs,
+                                   gp.stride, gp.phi0, gp.weight, gp.fft, gp.fdesc, gp.twiddle,
+                                   gp.wpow2, gp.P, gp.bhat, phase, ncm, job.mmax, job.flags,
+                                   gp.cls_bufA[cls], gp.cls_bufB[cls], fft_twcap(gp),
+                                   reinterpret_cast<T *const *>(maps_dev), map_lo, L.gbuf, L.npc,
+                                   L.nitems);
+  SHT_CUDA(cudaGetLastError());
+  if (L.gbuf) SHT_CUDA(cudaFreeAsync(L.gbuf, st));
+}
+
+template <typename T>
+void ring2phase_class(const JobDesc &job, const GeomPlan &gp, int cls, long long map_lo,
+                      const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
+                      cudaStream_t st) {
+  const FftLaunch L = plan_fft_launch(gp, cls, job.mmax, nmapptr, st);
+  auto k = ring2phase_kernel<T>;
+  SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L.smem)));
+  k<<<L.grid, L.thr, L.smem, st>>>(gp.cls_pairs + gp.cls_start[cls], gp.mlim, gp.nph, gp.ofs,
+                                   gp.stride, gp.phi0, gp.weight, gp.fft, gp.fdesc, gp.twiddle,
+                                   gp.wpow2, gp.P, gp.bhat, phase, ncm, job.mmax, job.flags,
+                                   gp.cls_bufA[cls], gp.cls_bufB[cls], fft_twcap(gp),
+                                   reinterpret_cast<const T *const *>(maps_dev), map_lo, L.gbuf,
+                                   L.npc, L.nitems);
+  SHT_CUDA(cudaGetLastError());
+  if (L.gbuf) SHT_CUDA(cudaFreeAsync(L.gbuf, st));
+}
+
+}  // namespace
 
 void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                        const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
@@ -706,25 +829,10 @@ void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, long long map_lo,
   ProfScope ps("ring_synth", st);
   for (int cls = 0; cls < int(gp.cls_N.size()); ++cls) {
     if (gp.cls_count[cls] == 0) continue;
-    dim3 grid(gp.cls_count[cls], nmapptr);
-    const size_t sm = fft_smem(gp, cls, job.mmax);
-    const int nbufA = gp.cls_bufA[cls], nbufB = gp.cls_bufB[cls];
-    const int thr = fft_threads(gp.cls_N[cls]);
-    const int *pairs = gp.cls_pairs + gp.cls_start[cls];
-    if (job.dp) {
-      auto k = phase2ring_kernel<double>;
-      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
-                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
-                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<double *const *>(maps_dev), map_lo);
-    } else {
-      auto k = phase2ring_kernel<float>;
-      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
-                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
-                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<float *const *>(maps_dev), map_lo);
-    }
-    SHT_CUDA(cudaGetLastError());
+    if (job.dp)
+      phase2ring_class<double>(job, gp, cls, map_lo, phase, ncm, maps_dev, nmapptr, st);
+    else
+      phase2ring_class<float>(job, gp, cls, map_lo, phase, ncm, maps_dev, nmapptr, st);
   }
 }
 
@@ -734,25 +842,10 @@ void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, long long map_lo,
   ProfScope ps("ring_anal", st);
   for (int cls = 0; cls < int(gp.cls_N.size()); ++cls) {
     if (gp.cls_count[cls] == 0) continue;
-    dim3 grid(gp.cls_count[cls], nmapptr);
-    const size_t sm = fft_smem(gp, cls, job.mmax);
-    const int nbufA = gp.cls_bufA[cls], nbufB = gp.cls_bufB[cls];
-    const int thr = fft_threads(gp.cls_N[cls]);
-    const int *pairs = gp.cls_pairs + gp.cls_start[cls];
-    if (job.dp) {
-      auto k = ring2phase_kernel<double>;
-      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
-                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
-                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<const double *const *>(maps_dev), map_lo);
-    } else {
-      auto k = ring2phase_kernel<float>;
-      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-      k<<<grid, thr, sm, st>>>(pairs, gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
-                               gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm,
-                               job.mmax, job.flags, nbufA, nbufB, reinterpret_cast<const float *const *>(maps_dev), map_lo);
-    }
-    SHT_CUDA(cudaGetLastError());
+    if (job.dp)
+      ring2phase_class<double>(job, gp, cls, map_lo, maps_dev, nmapptr, phase, ncm, st);
+    else
+      ring2phase_class<float>(job, gp, cls, map_lo, maps_dev, nmapptr, phase, ncm, st);
   }
 }
 

@@ -220,3 +220,32 @@ def test_mixed_spin2_analysis_geometries(spec, lmax, mmax):
     o64, omx = _anal_spin_both(spec, lmax, mmax, 2, 2, seed=21)
     for x, y in zip(omx, o64):
         assert rel_l2(x, y) < TOL
+
+
+def test_mixed_nside4096_lmax8192_round_trip():
+    # the large polarised configuration: Nside 4096 (rings up to 16384 pixels),
+    # lmax = mmax = 8192, spin 0 + 2, device-resident; mixed against FP64 in
+    # both directions
+    import torch
+    nside, lmax = 4096, 8192
+    g, a = sb.Geometry.healpix(nside), sb.AlmInfo.triangular(lmax, lmax)
+    dev = torch.device("cuda:0")
+    npix = 12 * nside * nside
+    for spin in (0, 2):
+        nc = 1 if spin == 0 else 2
+        alms = [torch.view_as_real(torch.from_numpy(
+            random_alm(lmax, lmax, seed=80 + i)).to(dev)).reshape(-1) for i in range(nc)]
+        m64 = [torch.zeros(npix, dtype=torch.float64, device=dev) for _ in range(nc)]
+        mmx = [torch.zeros_like(x) for x in m64]
+        sb.execute_device(sb.SHARP_ALM2MAP, spin, alms, m64, g, a, 1, DP)
+        sb.execute_device(sb.SHARP_ALM2MAP, spin, alms, mmx, g, a, 1, DP | MIXED)
+        a64 = [torch.zeros_like(x) for x in alms]
+        amx = [torch.zeros_like(x) for x in alms]
+        sb.execute_device(sb.SHARP_MAP2ALM, spin, a64, m64, g, a, 1, DP)
+        sb.execute_device(sb.SHARP_MAP2ALM, spin, amx, m64, g, a, 1, DP | MIXED)
+        torch.cuda.synchronize()
+        for x, y in zip(mmx, m64):
+            assert (torch.linalg.norm(x - y) / torch.linalg.norm(y)).item() < TOL
+        for x, y in zip(amx, a64):
+            assert (torch.linalg.norm(x - y) / torch.linalg.norm(y)).item() < TOL
+        del alms, m64, mmx, a64, amx

@@ -384,3 +384,48 @@ def test_device_pointer_entry_matches_host_entry():
     sb.execute_device(1, 0, [ta], [tm], g, a, 1, DP)
     torch.cuda.synchronize()
     assert np.array_equal(tm.cpu().numpy(), host)
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_long_rings_match_reference(ref, spin):
+    # rings too long for a shared-memory FFT (their buffers run in global
+    # scratch): a power-of-two length 16384, a Bluestein length 8194
+    # (8194/2 = 17 * 241) and a mixed-radix length 16380, with a few short
+    # rings in the same geometry; both directions, weights, phi0 shifts
+    lmax = 96
+    nph = np.array([16384, 8194, 16380, 16384, 30, 8194, 64, 16380], np.int32)
+    nr = len(nph)
+    theta = np.linspace(0.3, 2.8, nr)
+    ofs = np.concatenate([[0], np.cumsum(nph[:-1])]).astype(np.intp)
+    st = np.ones(nr, np.int32)
+    phi0 = np.linspace(0.0, 0.4, nr)
+    w = np.linspace(0.5, 1.5, nr)
+    g1 = sb.Geometry.general(nph, ofs, st, phi0, theta, w)
+    g2 = ref.general(nph, ofs, st, phi0, theta, w)
+    a1, a2 = sb.AlmInfo.triangular(lmax), ref.triangular(lmax, lmax)
+    npix = int(nph.sum())
+    na = _nalm(1, spin)
+    alms = [uniform_alm(lmax, seed=70 + i, spin=spin) for i in range(na)]
+    m1 = [np.zeros(npix) for _ in range(na)]
+    m2 = [np.zeros_like(x) for x in m1]
+    sb.execute(1, spin, [x.copy() for x in alms], m1, g1, a1, 1, DP)
+    ref.execute(1, spin, [x.copy() for x in alms], m2, g2, a2, 1, DP)
+    for x, y in zip(m1, m2):
+        assert rel_l2(x, y) < TOL
+    rng = np.random.default_rng(spin)
+    maps = [rng.standard_normal(npix) for _ in range(na)]
+    o1 = [np.zeros(sb.nalm_triangular(lmax), np.complex128) for _ in range(na)]
+    o2 = [x.copy() for x in o1]
+    sb.execute(0, spin, o1, [x.copy() for x in maps], g1, a1, 1, DP)
+    ref.execute(0, spin, o2, [x.copy() for x in maps], g2, a2, 1, DP)
+    for x, y in zip(o1, o2):
+        assert rel_l2(x, y) < TOL
+
+
+def test_healpix_nside4096_matches_reference(ref):
+    # Nside 4096 (rings up to 16384 pixels, the large-ring FFT path for the
+    # equatorial belt and the longest polar rings) at a small lmax
+    nside, lmax = 4096, 64
+    o1, o2 = run_pair(ref, ("healpix", nside), lmax, lmax, 0, 1, seed=4)
+    for x, y in zip(o1, o2):
+        assert rel_l2(x, y) < TOL
