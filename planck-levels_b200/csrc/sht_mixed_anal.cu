@@ -32,8 +32,10 @@
 //    values mu_l = lambda_l / c_l; c_l is applied when the a_lm are scattered.
 //
 // Warp roles: spin 0: 8 producer warps (256 ring pairs per group); spin s:
-// 4 producer warps (128 ring pairs, two recurrences each).  The last warp
-// (lane 0) stages each l-tile's recurrence coefficients into shared memory
+// 4 producer warps (128 ring pairs, two recurrences each).  Four flusher
+// warps (one per TMEM subpartition) read the class sums back and update the
+// output while the producers run the next tiles.  The last warp (lane 0)
+// stages each l-tile's recurrence coefficients into shared memory
 // (cp.async.bulk) and issues its MMAs.  Every wait is bounded; a timeout is
 // reported through the error word.
 #include <cuda_runtime.h>
@@ -67,7 +69,8 @@ struct AShape {
   static constexpr int TY = SPIN ? 2 : 1;              // recurrence values per pair and l
   static constexpr int PW = SPIN ? 4 : 8;              // producer warps
   static constexpr int G = 32 * PW;                    // ring pairs per group
-  static constexpr int THREADS = 32 * (PW + 1);
+  static constexpr int FW = 4;                         // flusher warps (one per TMEM subpartition)
+  static constexpr int THREADS = 32 * (PW + FW + 1);
   static constexpr int KB = 4 * TY * G;                // K bytes of a group
   static constexpr int KCM = 8 * TY;                   // K core matrices per warp slice
   static constexpr int SLICE = (KCM - 1) * kALBO + (kAM / 8) * 128;
@@ -126,17 +129,18 @@ __global__ void mixed_anal_coef_kernel(int lmax, int mmax, int spin,
 }
 
 // Reads back a pair of tiles of class sums (tiles 2f and 2f+1 of the group:
-// lanes 0-15 and 16-31 of this warp's subpartition, column set f & 1) and
-// adds the FP64 result to the output.  The five class sums of a column are
-// combined exactly in 64-bit integers: T = sum_w D_w 2^(8(w-2)).
+// lanes 0-15 and 16-31 of this warp's subpartition, TMEM column set `set`)
+// and adds the FP64 result to the output.  The five class sums of a column
+// are combined exactly in 64-bit integers: T = sum_w D_w 2^(8(w-2)).
 template <class S>
-__device__ __forceinline__ void flush_pair(uint32_t tmem, int f, int ntile, int l0, int lmax,
-                                           long long mo, const double2 *__restrict__ coef,
+__device__ __forceinline__ void flush_pair(uint32_t tmem, int set, int f, int ntile, int l0,
+                                           int lmax, long long mo,
+                                           const double2 *__restrict__ coef,
                                            const double *s_fscale, const double *s_corr,
                                            double2 *__restrict__ Aout, int ncA, int comp0,
                                            int warp, int lane) {
   const int k = warp & 3;
-  const uint32_t base = tmem + (uint32_t(32 * k) << 16) + uint32_t((f & 1) * S::NP);
+  const uint32_t base = tmem + (uint32_t(32 * k) << 16) + uint32_t(set * S::NP);
   const int t = 2 * f + (lane >> 4);
   const int l = l0 + t * kAM + 16 * k + (lane & 15);
   const bool row = t < ntile && l <= lmax;
@@ -173,6 +177,19 @@ __device__ __forceinline__ void flush_pair(uint32_t tmem, int f, int ntile, int 
   }
 }
 
+// Jobs run group-major (group g of ring pairs, l-tile t); tiles 2f, 2f+1 of a
+// group form pair P = g * npg + f (npg pairs per group), whose class sums
+// live in TMEM column set P mod 2.
+//
+// Barriers (all waits bounded):
+//   full_a[st]  producers -> issuer: A stage st holds job J's words
+//   done[st]    issuer -> producers: job J's MMAs are complete (A stage and,
+//               after a group's last job, B may be rewritten)
+//   cfull[st]   bulk copy -> producers: job J's coefficients are staged
+//   dfull[set]  issuer -> flushers: pair P's class sums are complete
+//   dfree[set]  flushers -> issuer: pair P has been read back
+//   sfull[sl]   producers -> flushers: the scales of group g (slot g mod 2)
+//   sfree[sl]   flushers -> producers: group g has been read back
 template <class S>
 __global__ void __launch_bounds__(S::THREADS, 1)
 mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
@@ -182,12 +199,14 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
                   const double2 *__restrict__ phase, int ncm, int pcomp0, int lmax, int ms,
                   double2 *__restrict__ Aout, int ncA, int comp0, int *__restrict__ err) {
   constexpr int PW = S::PW;
+  constexpr int FW = S::FW;                  // flusher warps PW .. PW+3
+  constexpr int LW = PW + FW;                // coefficient loader and MMA issuer
   extern __shared__ __align__(128) unsigned char sm[];
-  __shared__ uint64_t full_a[2], done[2], cfull[2];
+  __shared__ uint64_t full_a[2], done[2], cfull[2], dfull[2], dfree[2], sfull[2], sfree[2];
   __shared__ uint32_t tslot;
   __shared__ double s_red[PW][S::NH];
   __shared__ long long s_psum[PW][S::NH];
-  __shared__ double s_amax[S::NH], s_fscale[S::NH], s_corr[S::NH];
+  __shared__ double s_amax[S::NH], s_fscale[2][S::NH], s_corr[2][S::NH];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m = blockIdx.x;
@@ -195,6 +214,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
   const int cnt = count[m];
   const long long mo = moff[m] - m;
   const int ntile = mhi <= lmax ? (lmax - mhi + kAM) / kAM : 0;
+  const int npg = (ntile + 1) / 2;
   const int ngroup = (cnt + S::G - 1) / S::G;
   const int njobs = ngroup * ntile;
   unsigned char *sA = sm;
@@ -209,6 +229,10 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       mbar_init(&full_a[i], PW);
       mbar_init(&done[i], 1);
       mbar_init(&cfull[i], 1);
+      mbar_init(&dfull[i], 1);
+      mbar_init(&dfree[i], FW);
+      mbar_init(&sfull[i], 1);
+      mbar_init(&sfree[i], FW);
     }
     fence_mbar_init();
   }
@@ -221,7 +245,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
   tc_fence_after();
   const uint32_t tmem = tslot;
 
-  if (warp == PW) {
+  if (warp == LW) {
     // ------- coefficient loader and MMA issuer (lane 0 issues) -------
     auto load_coef = [&](int j) {
       const int l0 = mhi + (j % ntile) * kAM;
@@ -237,7 +261,12 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
     int issued = -1;
     for (int J = 0; J < njobs; ++J) {
       const int st = J & 1;
-      if (!__all_sync(0xffffffffu, mbar_wait(&full_a[st], (J >> 1) & 1))) {
+      const int g = J / ntile, t = J - g * ntile;
+      const int P = g * npg + (t >> 1), set = P & 1;
+      bool w = mbar_wait(&full_a[st], (J >> 1) & 1);
+      // the pair's column set is free once pair P-2 has been read back
+      if ((t & 1) == 0 && P >= 2) w = w && mbar_wait(&dfree[set], ((P >> 1) - 1) & 1);
+      if (!__all_sync(0xffffffffu, w)) {
         ok = false;
         break;
       }
@@ -245,9 +274,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       if (lane == 0) {
         // the producers are done with this job's coefficients
         if (J + 2 < njobs) load_coef(J + 2);
-        const int t = J % ntile;
-        const uint32_t d =
-            tmem + (uint32_t(16 * (t & 1)) << 16) + uint32_t(((t >> 1) & 1) * S::NP);
+        const uint32_t d = tmem + (uint32_t(16 * (t & 1)) << 16) + uint32_t(set * S::NP);
         const uint64_t a0 = make_desc(sA32 + st * PW * S::SLICE, kALBO, 128);
         // K-step k covers bytes [32k, 32k+32): warp slice k / (4 TY), core
         // matrices 2 (k mod 4 TY) and the next; the start-address field (bits
@@ -258,6 +285,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
                  a0 + uint64_t(((k / (4 * S::TY)) * S::SLICE + (k % (4 * S::TY)) * 2 * kALBO) >> 4),
                  b0 + uint64_t((2 * k * S::BLBO) >> 4), idesc, k > 0 ? 1u : 0u);
         mma_commit(&done[st]);
+        if ((t & 1) || t == ntile - 1) mma_commit(&dfull[set]);
       }
       __syncwarp();
       issued = J;
@@ -266,11 +294,33 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       if (lane == 0) *reinterpret_cast<volatile int *>(err) = 1;
       if (issued >= 0) mbar_wait(&done[issued & 1], (issued >> 1) & 1);
     }
+  } else if (warp >= PW) {
+    // ---- flushers: warp PW + k reads lanes 32k .. 32k+31 of every pair ----
+    bool ok = true;
+    for (int g = 0; g < ngroup; ++g) {
+      const int sl = g & 1;
+      if (ok) ok = __all_sync(0xffffffffu, mbar_wait(&sfull[sl], (g >> 1) & 1));
+      for (int f = 0; f < npg; ++f) {
+        const int P = g * npg + f;
+        if (ok) ok = __all_sync(0xffffffffu, mbar_wait(&dfull[P & 1], (P >> 1) & 1));
+        if (ok) {
+          tc_fence_after();
+          flush_pair<S>(tmem, P & 1, f, ntile, mhi, lmax, mo, coef, s_fscale[sl], s_corr[sl],
+                        Aout, ncA, comp0, warp, lane);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&dfree[P & 1]);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sfree[sl]);
+    }
+    if (!ok && lane == 0) *reinterpret_cast<volatile int *>(err) = 1;
   } else {
     // ---------------- producers: one ring pair per thread ----------------
     // All producer warps run the same loops (named barriers inside); a wait
-    // that gives up clears ok, after which the warp skips waits and reads of
-    // TMEM but keeps its place in the barriers.
+    // that gives up clears ok, after which the warp skips waits but keeps
+    // its place in the barriers.
     bool ok = true;
     // this pair's K segment of B: 4 TY bytes
     const uint32_t bcol = ((tid * 4 * S::TY) >> 4) * S::BLBO + ((tid * 4 * S::TY) & 15);
@@ -282,6 +332,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
     const double sgn_mfac = (m & 1) ? -pre_v[m] : pre_v[m];
     int J = 0;
     for (int g = 0; g < ngroup; ++g) {
+      const int sl = g & 1;
       const int p = g * S::G + tid;
       const bool valid = p < cnt;
       const bool has_s = valid && nph_ring[2 * p + 1] > 0;
@@ -330,7 +381,8 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         s_amax[tid] = a;
       }
       producers_sync<S::G>();
-      // quantise, write this pair's K segment of the Toeplitz B tile
+      // quantise, write this pair's K segment of the Toeplitz B tile (the
+      // MMAs of the previous group are complete: its last done was seen)
 #pragma unroll
       for (int i = 0; i < S::NH; ++i) {
         const double amax = s_amax[i];
@@ -367,16 +419,19 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         for (int o = 16; o; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
         if (lane == 0) s_psum[warp][i] = ps;
       }
+      // the scale slot of group g-2 is free once its pairs have been read back
+      if (g >= 2 && ok) ok = __all_sync(0xffffffffu, mbar_wait(&sfree[sl], ((g >> 1) - 1) & 1));
       producers_sync<S::G>();
       if (tid < S::NH) {
         long long ps = 0;
         for (int w = 0; w < PW; ++w) ps += s_psum[w][tid];
         // flush units: T = S / 2^16, so the offset correction is 2^15 sum q and
         // the scale amax / 2^44
-        s_corr[tid] = 32768.0 * double(ps);
-        s_fscale[tid] = s_amax[tid] * 0x1p-44;
+        s_corr[sl][tid] = 32768.0 * double(ps);
+        s_fscale[sl][tid] = s_amax[tid] * 0x1p-44;
       }
       producers_sync<S::G>();
+      if (tid == 0) mbar_arrive(&sfull[sl]);
 
       // recurrence seed(s) of this pair
       const double x = valid ? cth[p] : 0.0;
@@ -395,7 +450,6 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         live = spin_start(valid, x, valid ? sth[p] : 0.0, m, spin, pre_v[m], pre_e[m], mu0, mu1,
                           mm0, mm1, E, Em, act);
       }
-      int fnext = 0;   // next tile pair of this group to read back
       for (int t = 0; t < ntile; ++t, ++J) {
         const int st = J & 1;
         if (ok) {
@@ -403,15 +457,6 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
           bool w = J < 2 || mbar_wait(&done[st], ((J >> 1) - 1) & 1);
           w = w && mbar_wait(&cfull[st], (J >> 1) & 1);
           ok = __all_sync(0xffffffffu, w);
-          // tiles t-3, t-2 are complete once done(J-2) has been seen
-          if (ok && (t & 1) && t >= 3) {
-            if (PW == 4 || (warp >> 2) == (fnext & 1)) {
-              tc_fence_after();
-              flush_pair<S>(tmem, fnext, ntile, mhi, lmax, mo, coef, s_fscale, s_corr, Aout, ncA,
-                            comp0, warp, lane);
-            }
-            ++fnext;
-          }
         }
         const uint32_t slice = sA32 + (st * PW + warp) * S::SLICE +
                                (S::SPIN ? (lane >> 1) * kALBO + 8 * (lane & 1)
@@ -501,16 +546,9 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         __syncwarp();
         if (lane == 0) mbar_arrive(&full_a[st]);
       }
-      // end of the group: read back the pairs still in TMEM
+      // B is rewritten by the next group once the last MMA of this one is done
       if (ok && ntile > 0)
         ok = __all_sync(0xffffffffu, mbar_wait(&done[(J - 1) & 1], ((J - 1) >> 1) & 1));
-      for (; 2 * fnext < ntile; ++fnext)
-        if (ok && (PW == 4 || (warp >> 2) == (fnext & 1))) {
-          tc_fence_after();
-          flush_pair<S>(tmem, fnext, ntile, mhi, lmax, mo, coef, s_fscale, s_corr, Aout, ncA,
-                        comp0, warp, lane);
-        }
-      // B, the scales and the TMEM columns are reused by the next group
       tc_fence_before();
       producers_sync<S::G>();
       tc_fence_after();
