@@ -453,8 +453,7 @@ mixed_synth_kernel(const int2 *__restrict__ items, const int *__restrict__ count
     int E, Em = 0;
     bool act, live;
     if constexpr (S::T == 1) {
-      XD sd = valid ? xd_pow(sth[p], m) : XD{0.0, 0};
-      sd = xd_norm(sd.v * ((m & 1) ? -pre_v[m] : pre_v[m]), sd.e);
+      const XD sd = valid ? xd_pow_log(sth[p], m, (m & 1) ? -pre_v[m] : pre_v[m]) : XD{0.0, 0};
       mu0 = 0.0;
       mu1 = sd.v;
       E = sd.e;
@@ -462,8 +461,8 @@ mixed_synth_kernel(const int2 *__restrict__ items, const int *__restrict__ count
       act = live && E >= -kSwitchExp;
       if (act) mu1 = ldexp(mu1, E);
     } else {
-      live = spin_start(valid, x, valid ? sth[p] : 0.0, m, spin, pre_v[m], pre_e[m], mu0, mu1,
-                        mm0, mm1, E, Em, act);
+      live = spin_start_log(valid, x, valid ? sth[p] : 0.0, m, spin, pre_v[m], pre_e[m], mu0,
+                            mu1, mm0, mm1, E, Em, act);
     }
     for (int c = 0; c < nch; ++c) {
       const int sa = c % kSA, sb = c % kSB;

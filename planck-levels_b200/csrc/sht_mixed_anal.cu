@@ -439,16 +439,15 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       int E = 0, Em = 0;
       bool act, live;
       if constexpr (!S::SPIN) {
-        XD sd = valid ? xd_pow(sth[p], m) : XD{0.0, 0};
-        sd = xd_norm(sd.v * sgn_mfac, sd.e);
+        const XD sd = valid ? xd_pow_log(sth[p], m, sgn_mfac) : XD{0.0, 0};
         mu1 = sd.v;
         E = sd.e;
         live = valid && sd.v != 0.0;
         act = live && E >= -kSwitchExp;
         if (act) mu1 = ldexp(mu1, E);
       } else {
-        live = spin_start(valid, x, valid ? sth[p] : 0.0, m, spin, pre_v[m], pre_e[m], mu0, mu1,
-                          mm0, mm1, E, Em, act);
+        live = spin_start_log(valid, x, valid ? sth[p] : 0.0, m, spin, pre_v[m], pre_e[m], mu0,
+                              mu1, mm0, mm1, E, Em, act);
       }
       for (int t = 0; t < ntile; ++t, ++J) {
         const int st = J & 1;
