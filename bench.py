@@ -302,7 +302,12 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     synchronize on both sides), launch count and per-family kernel time."""
     if clk:
         clk.__enter__()
-        time.sleep(2.0)   # let nvidia-smi finish starting before the warm-up ends
+        # nvidia-smi's start-up stalls the GPU for about a second: wait until
+        # it samples (two lines) so the stall stays out of the timed region
+        t_end = time.time() + 15.0
+        while len(clk.lines) < 2 and time.time() < t_end and clk.proc is not None:
+            time.sleep(0.05)
+        time.sleep(0.5)
     lib.sharp_b200_profile(1)   # warm-up runs with the same event instrumentation
     for _ in range(warmup):
         fn()

@@ -10,34 +10,34 @@
 // the north/south parts of the combined Q/U phase factors of the two
 // Wigner-d recurrences (the even/odd factors of the FP64 kernel are
 // Hn +- Hs).  As in the synthesis, the FP64 recurrence stays on the CUDA
-// cores and the contraction runs exactly in integers on tcgen05.mma.kind::i8,
-// here with the roles of the operands turned around:
+// cores and the contraction runs exactly in integers on tcgen05.mma.kind::i8:
 //
-//  * A (M = 64 consecutive l, K = (ring pair, value, byte)): the words
+//  * A (tensor memory, M = 128 rows, K = (ring pair, value, byte)): the
+//    Toeplitz expansion of the signed base-256 digits of the group's phase
+//    factors, quantised per group of ring pairs and (half, column) against the
+//    group's maximum; row (hc, w) holds class w of (half, column) hc.  Built
+//    once per group, it stays in TMEM while the group sweeps all l, so the
+//    MMAs read only the B operand from shared memory.
+//  * B (shared memory, N = 64 consecutive l, K as A): the words
 //    u_l(p) = 2^31 + round(lambda_l(p) 2^30 / b_l) with the analytic bound
 //    b_l (sqrt((2l+1)/4pi) at spin 0; 1 for each of d^l_{m,+-s}), one
 //    magic-constant DFMA each; a producer thread owns one ring pair and
 //    writes one (spin: two) 4-byte words per l.
-//  * B (N = (half, column, weight), K as A): the Toeplitz expansion of the
-//    signed base-256 digits of the phase factors, quantised per group of ring
-//    pairs and (half, column) against the group's maximum.  It is built once
-//    per group in shared memory and stays there while the group sweeps all l.
-//  * D (int32, TMEM): per l-tile the exact class sums over the group's ring
-//    pairs.  Two tiles share one TMEM column set (lanes 0-15 and 16-31 of
-//    each subpartition), two sets alternate; a pair is read back one lane per
-//    l, its class sums combined exactly in 64-bit integers, corrected for the
-//    2^31 offset and scaled in FP64, and added to the output (one CTA per m,
-//    so no atomics).
+//  * D (int32, TMEM, 128 lanes x 64 columns per l-tile, two buffers): the
+//    exact class sums over the group's ring pairs.  A tile is read back
+//    through shared memory, its five class sums per (l, half, column)
+//    combined exactly in 64-bit integers, corrected for the 2^31 offset and
+//    scaled in FP64, and added to the output (one CTA per m: no atomics).
 //    Like the FP64 kernels, the output holds sums of the rescaled recurrence
 //    values mu_l = lambda_l / c_l; c_l is applied when the a_lm are scattered.
 //
-// Warp roles: spin 0: 8 producer warps (256 ring pairs per group); spin s:
-// 4 producer warps (128 ring pairs, two recurrences each).  Four flusher
-// warps (one per TMEM subpartition) read the class sums back and update the
-// output while the producers run the next tiles.  The last warp (lane 0)
-// stages each l-tile's recurrence coefficients into shared memory
-// (cp.async.bulk) and issues its MMAs.  Every wait is bounded; a timeout is
-// reported through the error word.
+// Warp roles: spin 0: 8 producer warps (256 ring pairs per group, up to 6
+// transforms per launch); spin s: 4 producer warps (128 ring pairs, two
+// recurrences each, up to 3 transforms).  Four flusher warps (one per TMEM
+// subpartition) read the class sums back and update the output while the
+// producers run the next tiles.  The last warp (lane 0) stages each l-tile's
+// recurrence coefficients into shared memory (cp.async.bulk) and issues its
+// MMAs.  Every wait is bounded; a timeout is reported through the error word.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -52,15 +52,21 @@ namespace sht {
 
 namespace {
 
-constexpr int kAM = 64;                       // l rows per tile (MMA M)
+constexpr int kAM = 64;                       // l per tile (MMA N)
 constexpr int kAClasses = 5;                  // byte-product weights 2^16 .. 2^48
-// A slice of one warp and tile (64 l x the warp's ring pairs, K-major, no
-// swizzle): the 8-row groups are contiguous (SBO = 128) and the K core
-// matrices lie kALBO = 8*128 + 16 bytes apart, so the per-l stores of a warp
-// spread over all 32 banks.
+constexpr int kHCW = 6;                       // (half, column) groups per TMEM subpartition
+// B slice of one producer warp and tile (64 l x the warp's ring pairs,
+// K-major, no swizzle): the 8-row groups are contiguous (SBO = 128) and the K
+// core matrices lie kALBO = 8*128 + 16 bytes apart, so the per-l stores of a
+// warp spread over all 32 banks.
 constexpr int kALBO = (kAM / 8) * 128 + 16;
+constexpr int kFRow = 4 * kAM + 16;           // flush staging row (bytes)
 
-constexpr int ceil16(int x) { return (x + 15) / 16 * 16; }
+// TMEM row (lane) of class w of (half, column) group hc: six groups of five
+// rows per 32-lane subpartition, so a subpartition holds whole groups.
+__host__ __device__ constexpr int arow(int hc, int w) {
+  return 32 * (hc / kHCW) + kAClasses * (hc % kHCW) + w;
+}
 
 template <bool SPIN_, int NB_>
 struct AShape {
@@ -68,28 +74,26 @@ struct AShape {
   static constexpr int NB = NB_;
   static constexpr int TY = SPIN ? 2 : 1;              // recurrence values per pair and l
   static constexpr int PW = SPIN ? 4 : 8;              // producer warps
+  static constexpr int FW = 4;                         // flusher warps (one per subpartition)
   static constexpr int G = 32 * PW;                    // ring pairs per group
-  static constexpr int FW = 4;                         // flusher warps (one per TMEM subpartition)
   static constexpr int THREADS = 32 * (PW + FW + 1);
   static constexpr int KB = 4 * TY * G;                // K bytes of a group
+  static constexpr int ACOLS = KB / 4;                 // TMEM columns of the A operand
   static constexpr int KCM = 8 * TY;                   // K core matrices per warp slice
   static constexpr int SLICE = (KCM - 1) * kALBO + (kAM / 8) * 128;
+  static constexpr int STAGES = 2 * PW * SLICE;        // both B stages
   static constexpr int CE = SPIN ? 32 : 16;            // coefficient bytes per l
   static constexpr int COEF = kAM * CE;                // one tile's coefficients
   static constexpr int OUT = SPIN ? 4 : 2;             // real outputs per transform
   static constexpr int NCOL = OUT * NB;
   static constexpr int NH = 2 * NCOL;                  // (half, column): north, then south
-  static constexpr int NPR = kAClasses * NH;           // B rows used
-  static constexpr int NP = ceil16(NPR);               // MMA N
-  // B (NP x KB): row groups contiguous, K core matrices BLBO apart
-  static constexpr int BLBO = (NP / 8) * 128 + 16;
-  static constexpr int BBYTES = ((KB / 16 - 1) * BLBO + (NP / 8) * 128 + 127) / 128 * 128;
-  static constexpr int SMEM = 2 * PW * SLICE + BBYTES + 2 * COEF;
-  // TMEM: a pair of tiles shares one column set (lane halves); two sets
-  static constexpr uint32_t NCOLS = 2 * NP <= 32 ? 32 : 2 * NP <= 64 ? 64 : 2 * NP <= 128 ? 128
-                                    : 2 * NP <= 256 ? 256 : 512;
+  static constexpr int AROW = KB + 16;                 // A staging row (bytes)
+  static constexpr int FLUSH = FW * 32 * kFRow;        // flush staging
+  static constexpr int SMEM = STAGES + FLUSH + 2 * COEF;
+  static constexpr uint32_t NCOLS = 512;               // A: 256 columns, D: 2 x 64
   static_assert(KB == 1024, "K extent of a group");
-  static_assert(NP <= 256 && 2 * NP <= 512, "TMEM / MMA N shape");
+  static_assert(NH <= 4 * kHCW, "(half, column) groups fit the four subpartitions");
+  static_assert(arow(4 * kHCW - 1, kAClasses - 1) * AROW + KB <= STAGES, "A staging");
   static_assert(SMEM + 4096 <= 232448, "shared memory");
 };
 
@@ -99,9 +103,53 @@ __device__ __forceinline__ void sts_u32(uint32_t a, uint32_t v) {
 __device__ __forceinline__ void sts_u32x2(uint32_t a, uint32_t x, uint32_t y) {
   asm volatile("st.shared.v2.b32 [%0], {%1, %2};" :: "r"(a), "r"(x), "r"(y) : "memory");
 }
+__device__ __forceinline__ uint4 lds_u32x4(uint32_t a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
 template <int N>
 __device__ __forceinline__ void producers_sync() {
   asm volatile("bar.sync 1, %0;" :: "n"(N) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void named_sync(int id) {
+  asm volatile("bar.sync %0, %1;" :: "r"(id), "n"(N) : "memory");
+}
+// 16 consecutive 32-bit columns of this thread's TMEM lane (store)
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+      :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]),
+         "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]),
+         "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// D[tmem] (+)= A(tmem) * B(smem)^T, kind::i8 (A signed, B unsigned), int32.
+__device__ __forceinline__ void mma_i8_tmem_a(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
+                                              uint32_t idesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :: "r"(d_tmem), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z),
+         "r"(z), "r"(z)
+      : "memory");
+}
+// Instruction descriptor: D s32, A s8, B u8, both K-major, M = m, N = n.
+__host__ __device__ constexpr uint32_t make_idesc_s8u8(int m, int n) {
+  return (2u << 4) | (1u << 7) | (0u << 10) | (uint32_t(n >> 3) << 17) |
+         (uint32_t(m >> 4) << 24);
 }
 
 // Per-m coefficient table of the analysis, for l = m .. lmax + kPad:
@@ -128,66 +176,17 @@ __global__ void mixed_anal_coef_kernel(int lmax, int mmax, int spin,
   }
 }
 
-// Reads back a pair of tiles of class sums (tiles 2f and 2f+1 of the group:
-// lanes 0-15 and 16-31 of this warp's subpartition, TMEM column set `set`)
-// and adds the FP64 result to the output.  The five class sums of a column
-// are combined exactly in 64-bit integers: T = sum_w D_w 2^(8(w-2)).
-template <class S>
-__device__ __forceinline__ void flush_pair(uint32_t tmem, int set, int f, int ntile, int l0,
-                                           int lmax, long long mo,
-                                           const double2 *__restrict__ coef,
-                                           const double *s_fscale, const double *s_corr,
-                                           double2 *__restrict__ Aout, int ncA, int comp0,
-                                           int warp, int lane) {
-  const int k = warp & 3;
-  const uint32_t base = tmem + (uint32_t(32 * k) << 16) + uint32_t(set * S::NP);
-  const int t = 2 * f + (lane >> 4);
-  const int l = l0 + t * kAM + 16 * k + (lane & 15);
-  const bool row = t < ntile && l <= lmax;
-  // the output entries and the row factor are fetched before the TMEM reads
-  double2 *out = Aout + (mo + (row ? l : l0)) * ncA + comp0;
-  double2 o[S::NCOL / 2];
-#pragma unroll
-  for (int j = 0; j < S::NCOL / 2; ++j) o[j] = row ? out[j] : make_double2(0.0, 0.0);
-  const double cq = !row ? 1.0 : S::SPIN ? __ldg(coef + 2 * (mo + l) + 1).x
-                                         : __ldg(coef + mo + l).y;
-  uint32_t v[S::NP];
-#pragma unroll
-  for (int q = 0; q < S::NP; q += 16) tmem_ld16(base + q, *reinterpret_cast<uint32_t(*)[16]>(v + q));
-  tmem_ld_wait();
-  if (!row) return;
-  // the output is sum_p mu_l phi (the scatter applies c_l): lambda was
-  // quantised as c_l mu_l 2^30 / b_l, so the row factor is b_l / c_l = 2^30 / cq_l
-  const double b = kQ / cq;
-  const double sg = ((l - l0) & 1) ? -b : b;
-  double R[S::NH];
-#pragma unroll
-  for (int h = 0; h < S::NH; ++h) {
-    const uint32_t *d = v + h * kAClasses;
-    const long long P = (long long)int(d[0]) + ((long long)int(d[1]) << 8) +
-                        ((long long)int(d[2]) << 16) + ((long long)int(d[3]) << 24);
-    const double Pd = __longlong_as_double(P + 0x4338000000000000LL) - 6755399441055744.0;
-    R[h] = (fma(i2d_exact(d[4]), 4294967296.0, Pd) - s_corr[h]) * s_fscale[h];
-  }
-#pragma unroll
-  for (int j = 0; j < S::NCOL / 2; ++j) {
-    o[j].x += b * R[2 * j] + sg * R[S::NCOL + 2 * j];
-    o[j].y += b * R[2 * j + 1] + sg * R[S::NCOL + 2 * j + 1];
-    out[j] = o[j];
-  }
-}
-
-// Jobs run group-major (group g of ring pairs, l-tile t); tiles 2f, 2f+1 of a
-// group form pair P = g * npg + f (npg pairs per group), whose class sums
-// live in TMEM column set P mod 2.
+// Jobs run group-major (group g of ring pairs, l-tile t), J = g * ntile + t;
+// the class sums of job J live in TMEM D buffer J mod 2.
 //
 // Barriers (all waits bounded):
-//   full_a[st]  producers -> issuer: A stage st holds job J's words
-//   done[st]    issuer -> producers: job J's MMAs are complete (A stage and,
-//               after a group's last job, B may be rewritten)
+//   full_a[st]  producers -> issuer: B stage st holds job J's words (and, for
+//               a group's first job, the group's A operand is in TMEM)
+//   done[st]    issuer -> producers: job J's MMAs are complete (B stage and,
+//               after a group's last job, A may be rewritten)
 //   cfull[st]   bulk copy -> producers: job J's coefficients are staged
-//   dfull[set]  issuer -> flushers: pair P's class sums are complete
-//   dfree[set]  flushers -> issuer: pair P has been read back
+//   dfull[d]    issuer -> flushers: job J's class sums are complete
+//   dfree[d]    flushers -> issuer: job J's class sums have been read
 //   sfull[sl]   producers -> flushers: the scales of group g (slot g mod 2)
 //   sfree[sl]   flushers -> producers: group g has been read back
 template <class S>
@@ -214,13 +213,12 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
   const int cnt = count[m];
   const long long mo = moff[m] - m;
   const int ntile = mhi <= lmax ? (lmax - mhi + kAM) / kAM : 0;
-  const int npg = (ntile + 1) / 2;
   const int ngroup = (cnt + S::G - 1) / S::G;
   const int njobs = ngroup * ntile;
-  unsigned char *sA = sm;
-  unsigned char *sB = sm + 2 * PW * S::SLICE;
-  unsigned char *sC = sB + S::BBYTES;
-  const uint32_t sA32 = smem_u32(sA), sB32 = smem_u32(sB), sC32 = smem_u32(sC);
+  unsigned char *sB = sm;                              // B stages; A staging at group start
+  unsigned char *sF = sm + S::STAGES;                  // flush staging
+  unsigned char *sC = sF + S::FLUSH;                   // coefficient stages
+  const uint32_t sB32 = smem_u32(sB), sF32 = smem_u32(sF), sC32 = smem_u32(sC);
   constexpr int CW = S::CE / 16;                       // double2 entries per l
   const double2 *cf = coef + CW * mo;                  // cf[CW l]: coefficients of l
 
@@ -243,7 +241,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = tslot;
+  const uint32_t tmem = tslot;                 // A: columns [0, 256); D: 256 + 64 d
 
   if (warp == LW) {
     // ------- coefficient loader and MMA issuer (lane 0 issues) -------
@@ -255,17 +253,14 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
     if (lane == 0)
       for (int j = 0; j < 2 && j < njobs; ++j) load_coef(j);
     __syncwarp();
-    constexpr uint32_t idesc = make_idesc_i8(kAM, S::NP);
-    const uint64_t b0 = make_desc(sB32, S::BLBO, 128);
+    constexpr uint32_t idesc = make_idesc_s8u8(128, kAM);
     bool ok = true;
     int issued = -1;
     for (int J = 0; J < njobs; ++J) {
       const int st = J & 1;
-      const int g = J / ntile, t = J - g * ntile;
-      const int P = g * npg + (t >> 1), set = P & 1;
       bool w = mbar_wait(&full_a[st], (J >> 1) & 1);
-      // the pair's column set is free once pair P-2 has been read back
-      if ((t & 1) == 0 && P >= 2) w = w && mbar_wait(&dfree[set], ((P >> 1) - 1) & 1);
+      // D buffer st is free once job J-2 has been read back
+      if (J >= 2) w = w && mbar_wait(&dfree[st], ((J >> 1) - 1) & 1);
       if (!__all_sync(0xffffffffu, w)) {
         ok = false;
         break;
@@ -274,18 +269,19 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       if (lane == 0) {
         // the producers are done with this job's coefficients
         if (J + 2 < njobs) load_coef(J + 2);
-        const uint32_t d = tmem + (uint32_t(16 * (t & 1)) << 16) + uint32_t(set * S::NP);
-        const uint64_t a0 = make_desc(sA32 + st * PW * S::SLICE, kALBO, 128);
-        // K-step k covers bytes [32k, 32k+32): warp slice k / (4 TY), core
-        // matrices 2 (k mod 4 TY) and the next; the start-address field (bits
-        // 0-13, 16-byte units) is advanced per K-step
+        const uint32_t d = tmem + uint32_t(S::ACOLS + st * kAM);
+        const uint64_t b0 = make_desc(sB32 + st * PW * S::SLICE, kALBO, 128);
+        // K-step k covers bytes [32k, 32k+32): A columns 8k .. 8k+7; B warp
+        // slice k / (4 TY), core matrices 2 (k mod 4 TY) and the next (the
+        // start-address field, 16-byte units, is advanced per K-step)
 #pragma unroll
         for (int k = 0; k < S::KB / 32; ++k)
-          mma_i8(d,
-                 a0 + uint64_t(((k / (4 * S::TY)) * S::SLICE + (k % (4 * S::TY)) * 2 * kALBO) >> 4),
-                 b0 + uint64_t((2 * k * S::BLBO) >> 4), idesc, k > 0 ? 1u : 0u);
+          mma_i8_tmem_a(d, tmem + uint32_t(8 * k),
+                        b0 + uint64_t(((k / (4 * S::TY)) * S::SLICE +
+                                       (k % (4 * S::TY)) * 2 * kALBO) >> 4),
+                        idesc, k > 0 ? 1u : 0u);
         mma_commit(&done[st]);
-        if ((t & 1) || t == ntile - 1) mma_commit(&dfull[set]);
+        mma_commit(&dfull[st]);
       }
       __syncwarp();
       issued = J;
@@ -295,22 +291,79 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       if (issued >= 0) mbar_wait(&done[issued & 1], (issued >> 1) & 1);
     }
   } else if (warp >= PW) {
-    // ---- flushers: warp PW + k reads lanes 32k .. 32k+31 of every pair ----
+    // ---- flushers: warp PW + k reads lanes 32k .. 32k+31 of each tile ----
+    const int k = warp - PW;                   // == warp mod 4: its TMEM subpartition
+    const int ft = tid - 32 * PW;              // 0 .. 127
+    constexpr int kItems = (kAM * (S::NCOL / 2) + 32 * FW - 1) / (32 * FW);
+    const uint32_t frow = sF32 + (32 * k + lane) * kFRow;
     bool ok = true;
+    int J = 0;
     for (int g = 0; g < ngroup; ++g) {
       const int sl = g & 1;
       if (ok) ok = __all_sync(0xffffffffu, mbar_wait(&sfull[sl], (g >> 1) & 1));
-      for (int f = 0; f < npg; ++f) {
-        const int P = g * npg + f;
-        if (ok) ok = __all_sync(0xffffffffu, mbar_wait(&dfull[P & 1], (P >> 1) & 1));
+      const double *fsc = s_fscale[sl], *fco = s_corr[sl];
+      for (int t = 0; t < ntile; ++t, ++J) {
+        const int d = J & 1;
+        // items (l, complex output jo), real columns 2 jo, 2 jo + 1 of both
+        // halves: their output entries and row factors do not depend on the
+        // class sums, so they are fetched before the wait
+        const int l0 = mhi + t * kAM;
+        double2 po[kItems];
+        double pcq[kItems];
+#pragma unroll
+        for (int u = 0; u < kItems; ++u) {
+          const int it = ft + u * 32 * FW;
+          const int l = l0 + (it & (kAM - 1));
+          const bool v = ok && it < kAM * (S::NCOL / 2) && l <= lmax;
+          po[u] = v ? Aout[(mo + l) * ncA + comp0 + it / kAM] : make_double2(0.0, 0.0);
+          pcq[u] = !v ? 1.0 : S::SPIN ? __ldg(coef + 2 * (mo + l) + 1).x : __ldg(coef + mo + l).y;
+        }
+        if (ok) ok = __all_sync(0xffffffffu, mbar_wait(&dfull[d], (J >> 1) & 1));
+        // staging of the previous tile is no longer read
+        named_sync<32 * FW>(2);
         if (ok) {
           tc_fence_after();
-          flush_pair<S>(tmem, P & 1, f, ntile, mhi, lmax, mo, coef, s_fscale[sl], s_corr[sl],
-                        Aout, ncA, comp0, warp, lane);
+          uint32_t v[kAM];
+#pragma unroll
+          for (int q = 0; q < kAM; q += 16)
+            tmem_ld16(tmem + (uint32_t(32 * k) << 16) + uint32_t(S::ACOLS + d * kAM + q),
+                      *reinterpret_cast<uint32_t(*)[16]>(v + q));
+          tmem_ld_wait();
+#pragma unroll
+          for (int q = 0; q < kAM; q += 4) sts_u32x4(frow + 4 * q, v[q], v[q + 1], v[q + 2], v[q + 3]);
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&dfree[P & 1]);
+        if (lane == 0) mbar_arrive(&dfree[d]);
+        named_sync<32 * FW>(2);
+        if (ok) {
+#pragma unroll
+          for (int u = 0; u < kItems; ++u) {
+            const int it = ft + u * 32 * FW;
+            const int li = it & (kAM - 1), jo = it / kAM;
+            const int l = l0 + li;
+            if (it >= kAM * (S::NCOL / 2) || l > lmax) continue;
+            double R[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int hc = (e >> 1) * S::NCOL + 2 * jo + (e & 1);
+              uint32_t c[kAClasses];
+#pragma unroll
+              for (int w = 0; w < kAClasses; ++w) c[w] = lds_u32(sF32 + arow(hc, w) * kFRow + 4 * li);
+              const long long P = (long long)int(c[0]) + ((long long)int(c[1]) << 8) +
+                                  ((long long)int(c[2]) << 16) + ((long long)int(c[3]) << 24);
+              const double Pd = __longlong_as_double(P + 0x4338000000000000LL) - 6755399441055744.0;
+              R[e] = (fma(i2d_exact(c[4]), 4294967296.0, Pd) - fco[hc]) * fsc[hc];
+            }
+            // lambda was quantised as c_l mu_l 2^30 / b_l: row factor b_l / c_l = 2^30 / cq_l
+            const double b = kQ / pcq[u];
+            const double sg = ((l - mhi) & 1) ? -b : b;
+            double2 o = po[u];
+            o.x += b * R[0] + sg * R[2];
+            o.y += b * R[1] + sg * R[3];
+            Aout[(mo + l) * ncA + comp0 + jo] = o;
+          }
+        }
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&sfree[sl]);
@@ -322,14 +375,9 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
     // that gives up clears ok, after which the warp skips waits but keeps
     // its place in the barriers.
     bool ok = true;
-    // this pair's K segment of B: 4 TY bytes
-    const uint32_t bcol = ((tid * 4 * S::TY) >> 4) * S::BLBO + ((tid * 4 * S::TY) & 15);
-    for (int r = S::NPR; r < S::NP; ++r) {  // unused B rows stay zero
-      const uint32_t a = sB32 + (r >> 3) * 128 + (r & 7) * 16 + bcol;
-      if constexpr (S::SPIN) sts_u32x2(a, 0u, 0u); else sts_u32(a, 0u);
-    }
     const double flip = ((mhi - m + spin) & 1) ? -1.0 : 1.0;
     const double sgn_mfac = (m & 1) ? -pre_v[m] : pre_v[m];
+    const int sp = warp & 3;                   // this warp's TMEM subpartition
     int J = 0;
     for (int g = 0; g < ngroup; ++g) {
       const int sl = g & 1;
@@ -381,8 +429,8 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         s_amax[tid] = a;
       }
       producers_sync<S::G>();
-      // quantise, write this pair's K segment of the Toeplitz B tile (the
-      // MMAs of the previous group are complete: its last done was seen)
+      // quantise; the A words of this pair go to the staging rows (the B
+      // stages are free: the previous group's last MMA has completed)
 #pragma unroll
       for (int i = 0; i < S::NH; ++i) {
         const double amax = s_amax[i];
@@ -409,9 +457,8 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
           }
         }
 #pragma unroll
-        for (int w = 0; w < 5; ++w) {
-          const int row = i * kAClasses + w;
-          const uint32_t a = sB32 + (row >> 3) * 128 + (row & 7) * 16 + bcol;
+        for (int w = 0; w < kAClasses; ++w) {
+          const uint32_t a = sB32 + arow(i, w) * S::AROW + 4 * S::TY * tid;
           if constexpr (S::SPIN) sts_u32x2(a, word[0][w], word[S::TY - 1][w]);
           else sts_u32(a, word[0][w]);
         }
@@ -419,7 +466,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         for (int o = 16; o; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
         if (lane == 0) s_psum[warp][i] = ps;
       }
-      // the scale slot of group g-2 is free once its pairs have been read back
+      // the scale slot of group g-2 is free once its tiles have been read back
       if (g >= 2 && ok) ok = __all_sync(0xffffffffu, mbar_wait(&sfree[sl], ((g >> 1) - 1) & 1));
       producers_sync<S::G>();
       if (tid < S::NH) {
@@ -430,6 +477,28 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         s_corr[sl][tid] = 32768.0 * double(ps);
         s_fscale[sl][tid] = s_amax[tid] * 0x1p-44;
       }
+      // A rows of this warp's subpartition (lane = row) into TMEM; the PW / 4
+      // warps of a subpartition split the columns
+      {
+        constexpr int per = S::ACOLS / (PW / 4);
+        const int c0 = (warp >> 2) * per;
+        const uint32_t src = sB32 + (32 * sp + lane) * S::AROW + 4 * c0;
+        const uint32_t dst = tmem + (uint32_t(32 * sp) << 16) + uint32_t(c0);
+#pragma unroll 1
+        for (int c = 0; c < per; c += 16) {
+          uint32_t wv[16];
+#pragma unroll
+          for (int q = 0; q < 16; q += 4) {
+            // lanes 30, 31 of a subpartition are padding rows (zero)
+            const uint4 x = lane < kAClasses * kHCW ? lds_u32x4(src + 4 * (c + q))
+                                                    : make_uint4(0u, 0u, 0u, 0u);
+            wv[q] = x.x; wv[q + 1] = x.y; wv[q + 2] = x.z; wv[q + 3] = x.w;
+          }
+          tmem_st16(dst + uint32_t(c), wv);
+        }
+        tmem_st_wait();
+      }
+      tc_fence_before();
       producers_sync<S::G>();
       if (tid == 0) mbar_arrive(&sfull[sl]);
 
@@ -452,12 +521,12 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
       for (int t = 0; t < ntile; ++t, ++J) {
         const int st = J & 1;
         if (ok) {
-          // A stage of job J-2 is reused; this job's coefficients are staged
+          // B stage of job J-2 is reused; this job's coefficients are staged
           bool w = J < 2 || mbar_wait(&done[st], ((J >> 1) - 1) & 1);
           w = w && mbar_wait(&cfull[st], (J >> 1) & 1);
           ok = __all_sync(0xffffffffu, w);
         }
-        const uint32_t slice = sA32 + (st * PW + warp) * S::SLICE +
+        const uint32_t slice = sB32 + (st * PW + warp) * S::SLICE +
                                (S::SPIN ? (lane >> 1) * kALBO + 8 * (lane & 1)
                                         : (lane >> 2) * kALBO + 4 * (lane & 3));
         const uint32_t cs = sC32 + st * S::COEF;
@@ -545,7 +614,8 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
         __syncwarp();
         if (lane == 0) mbar_arrive(&full_a[st]);
       }
-      // B is rewritten by the next group once the last MMA of this one is done
+      // A (TMEM) and the staging rows are rewritten by the next group once
+      // the last MMA of this one is done
       if (ok && ntile > 0)
         ok = __all_sync(0xffffffffu, mbar_wait(&done[(J - 1) & 1], ((J - 1) >> 1) & 1));
       tc_fence_before();
@@ -598,17 +668,22 @@ void launch_mixed_anal(const JobDesc &job, const GeomPlan &gp, CoefPlan &cp,
   for (int t0 = 0; t0 < job.ntrans;) {
     int nb;
     if (job.spin == 0) {
-      nb = std::min(job.ntrans - t0, 4);
+      nb = std::min(job.ntrans - t0, 6);
       switch (nb) {
+        case 6: launch_anal_shape<AShape<false, 6>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
+        case 5: launch_anal_shape<AShape<false, 5>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
         case 4: launch_anal_shape<AShape<false, 4>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
         case 3: launch_anal_shape<AShape<false, 3>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
         case 2: launch_anal_shape<AShape<false, 2>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
         default: launch_anal_shape<AShape<false, 1>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
       }
     } else {
-      nb = std::min(job.ntrans - t0, 2);
-      if (nb == 2) launch_anal_shape<AShape<true, 2>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st);
-      else launch_anal_shape<AShape<true, 1>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st);
+      nb = std::min(job.ntrans - t0, 3);
+      switch (nb) {
+        case 3: launch_anal_shape<AShape<true, 3>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
+        case 2: launch_anal_shape<AShape<true, 2>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
+        default: launch_anal_shape<AShape<true, 1>>(job, gp, cp, phase, ncm, t0, Aout, ncA, d_err, st); break;
+      }
     }
     t0 += nb;
   }
