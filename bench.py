@@ -316,7 +316,12 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
         dist.barrier()
     torch.cuda.synchronize()
     l0 = lib.sharp_b200_kernel_launches()
-    lib.sharp_b200_profile(1)   # clears the warm-up spans
+    # per-family totals of the warm-up, subtracted below (the instrumentation
+    # stays as it is across the start of the timed region)
+    base = {}
+    for name in FAMILIES:
+        n = C.c_ulonglong(0)
+        base[name] = (lib.sharp_b200_profile_ms(name.encode(), C.byref(n)), n.value)
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     if clk:
         clk.mark()
@@ -334,8 +339,8 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     for name in FAMILIES:
         n = C.c_ulonglong(0)
         ms = lib.sharp_b200_profile_ms(name.encode(), C.byref(n))
-        if n.value:
-            fam[name] = (ms, n.value)
+        if n.value > base[name][1]:
+            fam[name] = (ms - base[name][0], n.value - base[name][1])
     lib.sharp_b200_profile(0)
     step_s = evs[0].elapsed_time(evs[-1]) * 1e-3 / steps
     per_step = [round(evs[i].elapsed_time(evs[i + 1]), 2) for i in range(steps)]

@@ -32,7 +32,7 @@ struct FftDesc {
   int rad[kMaxRadices];
   int blue;     // 1: Bluestein convolution of power-of-two length M
   int M;
-  long long bhat;  // offset of the transformed chirp (bit-reversed, /M)
+  long long bhat;  // offset of the transformed chirp (digit order of the DIF stages, /M)
 };
 
 // Per-geometry device tables (pairs in internal mlim order).

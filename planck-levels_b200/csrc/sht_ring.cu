@@ -200,46 +200,88 @@ __device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv, 
 // ---------------------------------------------------------------------------
 // Bluestein transform for lengths with large prime factors:
 // X_k = c_k sum_j (x_j c_j) conj(c_{k-j}), c_j = exp(-pi i j^2/N), evaluated
-// as a power-of-two convolution of length M >= 2N-1: in-place radix-2
-// decimation-in-frequency (bit-reversed output), product with the chirp
-// transform precomputed in the same order, decimation-in-time back to
+// as a power-of-two convolution of length M >= 2N-1: in-place radix-4
+// decimation in frequency (digit-reversed output), product with the chirp
+// transform precomputed in the same order, the inverse stages back to
 // natural order.  The inverse transform is conj(forward(conj x)).
 // ---------------------------------------------------------------------------
 template <class TW>
 __device__ __forceinline__ double2 chirp_of(int j, int n, int N, const TW &Wn) {
-  if ((n & 1) == 0) return Wn(int(((long long)j * j) % n));  // exp(-2 pi i (j^2 mod n)/n)
+  // j < N <= n <= 2^15, so j^2 fits 32 bits
+  const unsigned jj = unsigned(j) * unsigned(j);
+  if ((n & 1) == 0) return Wn(int(jj % unsigned(n)));  // exp(-2 pi i (j^2 mod n)/n)
   double sn, cs;
-  sincospi(-double(((long long)j * j) % (2ll * n)) / n, &sn, &cs);
+  sincospi(-double(jj % (2u * unsigned(n))) / n, &sn, &cs);
   return make_double2(cs, sn);
 }
 
+// In-place decimation in frequency of length M = 2^lg (output in the
+// digit order of the stages): one radix-2 stage when lg is odd, then radix-4
+// stages.  A stage of length len maps x_{i + j len/4} (j < 4) to
+// y_r = W_len^{ir} sum_j x_{i + j len/4} (-i)^{jr}, stored at i + r len/4.
 template <class TW>
 __device__ void dif_inplace(double2 *a, int M, const TW &Wp, int P) {
-  int lg = 31 - __clz(M);
-  for (int len = M; len >= 2; len >>= 1, --lg) {
+  const int lg = 31 - __clz(M);
+  int len = M;
+  if (lg & 1) {
     const int half = len >> 1, st = P / len;
-    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
-      const int blk = t >> (lg - 1), i = t & (half - 1);
-      const int b0 = blk * len + i;
-      const double2 u = a[b0], v = a[b0 + half];
-      a[b0] = cadd(u, v);
-      a[b0 + half] = cmul(csub(u, v), Wp(i * st));
+    for (int t = threadIdx.x; t < half; t += blockDim.x) {
+      const double2 u = a[t], v = a[t + half];
+      a[t] = cadd(u, v);
+      a[t + half] = cmul(csub(u, v), Wp(t * st));
+    }
+    __syncthreads();
+    len = half;
+  }
+  for (; len >= 4; len >>= 2) {
+    const int q = len >> 2, st = P / len, lq = 31 - __clz(q);
+    for (int t = threadIdx.x; t < (M >> 2); t += blockDim.x) {
+      const int i = t & (q - 1);
+      const int b0 = (t >> lq) * len + i;
+      const double2 x0 = a[b0], x1 = a[b0 + q], x2 = a[b0 + 2 * q], x3 = a[b0 + 3 * q];
+      const double2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
+      const double2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
+      const double2 md13 = make_double2(d13.y, -d13.x);  // -i (x1 - x3)
+      a[b0] = cadd(s02, s13);
+      a[b0 + q] = cmul(cadd(d02, md13), Wp(i * st));
+      a[b0 + 2 * q] = cmul(csub(s02, s13), Wp(2 * i * st));
+      a[b0 + 3 * q] = cmul(csub(d02, md13), Wp(3 * i * st));
     }
     __syncthreads();
   }
 }
 
+// Inverse of dif_inplace (conjugate twiddles, unnormalised): the stages in
+// reverse order, each mapping its digit order back to natural order.
 template <class TW>
 __device__ void dit_inplace_inv(double2 *a, int M, const TW &Wp, int P) {
-  int lg = 1;
-  for (int len = 2; len <= M; len <<= 1, ++lg) {
-    const int half = len >> 1, st = P / len;
-    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
-      const int blk = t >> (lg - 1), i = t & (half - 1);
-      const int b0 = blk * len + i;
-      const double2 u = a[b0], v = cmul(a[b0 + half], cconj(Wp(i * st)));
-      a[b0] = cadd(u, v);
-      a[b0 + half] = csub(u, v);
+  const int lg = 31 - __clz(M);
+  const int top = (lg & 1) ? (M >> 1) : M;
+  for (int len = 4; len <= top; len <<= 2) {
+    const int q = len >> 2, st = P / len, lq = 31 - __clz(q);
+    for (int t = threadIdx.x; t < (M >> 2); t += blockDim.x) {
+      const int i = t & (q - 1);
+      const int b0 = (t >> lq) * len + i;
+      const double2 z0 = a[b0];
+      const double2 z1 = cmul(a[b0 + q], cconj(Wp(i * st)));
+      const double2 z2 = cmul(a[b0 + 2 * q], cconj(Wp(2 * i * st)));
+      const double2 z3 = cmul(a[b0 + 3 * q], cconj(Wp(3 * i * st)));
+      const double2 s02 = cadd(z0, z2), d02 = csub(z0, z2);
+      const double2 s13 = cadd(z1, z3), d13 = csub(z1, z3);
+      const double2 pd13 = make_double2(-d13.y, d13.x);  // i (z1 - z3)
+      a[b0] = cadd(s02, s13);
+      a[b0 + q] = cadd(d02, pd13);
+      a[b0 + 2 * q] = csub(s02, s13);
+      a[b0 + 3 * q] = csub(d02, pd13);
+    }
+    __syncthreads();
+  }
+  if (lg & 1) {
+    const int half = M >> 1, st = P / M;
+    for (int t = threadIdx.x; t < half; t += blockDim.x) {
+      const double2 u = a[t], v = cmul(a[t + half], cconj(Wp(t * st)));
+      a[t] = cadd(u, v);
+      a[t + half] = csub(u, v);
     }
     __syncthreads();
   }
