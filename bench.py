@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import os
 import statistics
@@ -325,11 +326,16 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     if clk:
         clk.mark()
+    # a full Python garbage collection costs ~0.4 s of host time in this
+    # process: run it here and keep the collector off while timing
+    gc.collect()
+    gc.disable()
     evs[0].record(stream)
     for i in range(steps):
         fn()
         evs[i + 1].record(stream)
     torch.cuda.synchronize()
+    gc.enable()
     if clk:
         clk.__exit__()
     if dist:
@@ -449,10 +455,13 @@ def main():
     host_step()
     if dist:
         dist.barrier()
+    gc.collect()
+    gc.disable()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         host_step()
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    gc.enable()
     if dist:
         tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
