@@ -708,6 +708,158 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
   if (time) *time = wall_now() - t0;
 }
 
+// ---------------------------------------------------------------------------
+// Host-array jobs with several transforms: the transforms run in pieces so
+// that the host->device copies of piece k+1 and the device->host copies of
+// piece k-1 overlap the compute of piece k (three streams, event-ordered).
+// Each piece is an ordinary device-pointer job on window buffers; every
+// transform's arithmetic is that of the single-call path, so the results
+// are the same.  Returns false (nothing done) where the plain path applies.
+// ---------------------------------------------------------------------------
+cudaStream_t copy_stream(int which) {
+  static std::map<std::pair<int, int>, cudaStream_t> streams;
+  int dev = 0;
+  SHT_CUDA(cudaGetDevice(&dev));
+  auto key = std::make_pair(dev, which);
+  auto it = streams.find(key);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  SHT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  streams[key] = s;
+  return s;
+}
+
+bool execute_pipelined(sharp_jobtype type, int spin, void *alm, void *map,
+                       const sharp_geom_info *ginfo, const sharp_alm_info *ainfo, int ntrans,
+                       int flags, double *time, unsigned long long *opcnt) {
+  if (type != SHARP_ALM2MAP && type != SHARP_MAP2ALM) return false;
+  if (flags & (SHARP_ADJOINT | SHARP_NO_FFT)) return false;
+  if (!ginfo || !ainfo || !alm || !map || ntrans < 2 || ntrans > kMaxTrans) return false;
+  if (spin < 0 || spin > ainfo->lmax || ainfo->nm < 1 || ainfo->nm - 1 > ainfo->lmax) return false;
+  {
+    // every m exactly once (otherwise the plain path reports the error)
+    std::vector<char> seen(ainfo->nm, 0);
+    for (int i = 0; i < ainfo->nm; ++i) {
+      const int mv = ainfo->mval[i];
+      if (mv < 0 || mv >= ainfo->nm || seen[mv]) return false;
+      seen[mv] = 1;
+    }
+  }
+  const bool analysis = type == SHARP_MAP2ALM;
+  // piece size: the transforms one launch of the batched kernels takes
+  const int piece = spin > 0 ? 3 : (analysis ? 6 : 4);
+  if (ntrans <= piece) return false;
+  const double t0 = wall_now();
+  const int ncomp = spin > 0 ? 2 : 1;       // maps and a_lm per transform
+  const bool dp = (flags & SHARP_DP) != 0;
+  long long map_lo, map_hi, alm_lo, alm_hi;
+  bool map_covered, alm_covered, packed;
+  cudaStream_t cs = library_stream();
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mutex);
+    retain_pool_memory();
+    const int mmax = ainfo->nm - 1;
+    GeomPlan *gp = get_geom_plan(ginfo, ainfo->lmax, mmax, spin, cs);
+    AlmPlan *ap = get_alm_plan(ainfo, mmax, cs);
+    map_lo = gp->map_lo; map_hi = gp->map_hi; map_covered = gp->map_covered;
+    alm_lo = ap->lo; alm_hi = ap->hi; alm_covered = ap->covered; packed = ap->packed;
+  }
+  const size_t esz_map = dp ? 8 : 4, esz_alm = (dp ? 8 : 4) * (packed ? 1 : 2);
+  const long long map_n = map_hi - map_lo, alm_n = alm_hi - alm_lo;
+  const bool load_maps = analysis || (flags & SHARP_ADD) || !map_covered;
+  const bool load_alm = !analysis || (flags & SHARP_ADD) || !alm_covered;
+  void **alm_in = static_cast<void **>(alm);
+  void **map_in = static_cast<void **>(map);
+  cudaStream_t sin = copy_stream(0), sout = copy_stream(1);
+
+  // window buffers of one piece, released on the output stream after its copies
+  struct Piece {
+    std::vector<void *> dmap, dalm;
+    cudaEvent_t in_done = nullptr, compute_done = nullptr;
+  };
+  std::vector<Piece> pieces;
+  auto release = [&]() {
+    for (auto &pc : pieces) {
+      for (void *p : pc.dmap) if (p) cudaFreeAsync(p, sout);
+      for (void *p : pc.dalm) if (p) cudaFreeAsync(p, sout);
+      if (pc.in_done) cudaEventDestroy(pc.in_done);
+      if (pc.compute_done) cudaEventDestroy(pc.compute_done);
+    }
+    pieces.clear();
+  };
+  unsigned long long first_ops = 0;
+  try {
+    for (int t0p = 0; t0p < ntrans; t0p += piece) {
+      const int nt = std::min(piece, ntrans - t0p);
+      pieces.emplace_back();
+      Piece &pc = pieces.back();
+      pc.dmap.assign(size_t(nt) * ncomp, nullptr);
+      pc.dalm.assign(size_t(nt) * ncomp, nullptr);
+      SHT_CUDA(cudaEventCreateWithFlags(&pc.in_done, cudaEventDisableTiming));
+      SHT_CUDA(cudaEventCreateWithFlags(&pc.compute_done, cudaEventDisableTiming));
+      // inputs of the piece: host -> device on the input stream
+      for (int i = 0; i < nt * ncomp; ++i) {
+        const int gi = t0p * ncomp + i;
+        SHT_CUDA(cudaMallocAsync(&pc.dmap[i], esz_map * std::max<long long>(map_n, 1), sin));
+        SHT_CUDA(cudaMallocAsync(&pc.dalm[i], esz_alm * std::max<long long>(alm_n, 1), sin));
+        if (load_maps && map_n > 0)
+          SHT_CUDA(cudaMemcpyAsync(pc.dmap[i], static_cast<char *>(map_in[gi]) + esz_map * map_lo,
+                                   esz_map * map_n, cudaMemcpyHostToDevice, sin));
+        if (load_alm && alm_n > 0)
+          SHT_CUDA(cudaMemcpyAsync(pc.dalm[i], static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
+                                   esz_alm * alm_n, cudaMemcpyHostToDevice, sin));
+      }
+      SHT_CUDA(cudaEventRecord(pc.in_done, sin));
+      // compute on the library stream: a device-pointer job whose array
+      // bases are placed so that element lo sits at the start of each window
+      SHT_CUDA(cudaStreamWaitEvent(cs, pc.in_done, 0));
+      std::vector<void *> bm(nt * ncomp), ba(nt * ncomp);
+      for (int i = 0; i < nt * ncomp; ++i) {
+        bm[i] = static_cast<char *>(pc.dmap[i]) - esz_map * map_lo;
+        ba[i] = static_cast<char *>(pc.dalm[i]) - esz_alm * alm_lo;
+      }
+      unsigned long long oc = 0;
+      execute_impl(type, spin, ba.data(), bm.data(), ginfo, ainfo, nt, flags, true, cs, nullptr,
+                   &oc);
+      if (t0p == 0) first_ops = oc;
+      SHT_CUDA(cudaEventRecord(pc.compute_done, cs));
+      // outputs of the piece: device -> host on the output stream
+      SHT_CUDA(cudaStreamWaitEvent(sout, pc.compute_done, 0));
+      for (int i = 0; i < nt * ncomp; ++i) {
+        const int gi = t0p * ncomp + i;
+        if (analysis) {
+          if (alm_n > 0)
+            SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
+                                     pc.dalm[i], esz_alm * alm_n, cudaMemcpyDeviceToHost, sout));
+        } else if (map_n > 0) {
+          SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(map_in[gi]) + esz_map * map_lo,
+                                   pc.dmap[i], esz_map * map_n, cudaMemcpyDeviceToHost, sout));
+        }
+      }
+    }
+    release();
+    SHT_CUDA(cudaStreamSynchronize(sout));
+    SHT_CUDA(cudaStreamSynchronize(cs));
+    if (flags & SHARP_MIXED) check_tc_error();
+  } catch (const Failure &) {
+    release();
+    cudaStreamSynchronize(sout);
+    cudaStreamSynchronize(cs);
+    throw;
+  }
+  if (opcnt) {
+    // the count of one call with all transforms (per-triple weight of
+    // sharp_core_inc2.c:173,442): the pieces share the triples
+    const int n0 = std::min(piece, ntrans);
+    const unsigned long long c0 = spin == 0 ? 4 + 4ull * n0 : 12 + 16ull * n0;
+    const unsigned long long c = spin == 0 ? 4 + 4ull * ntrans : 12 + 16ull * ntrans;
+    const unsigned long long tot = ntrans > 0 ? first_ops / c0 : 0;
+    *opcnt = tot * c;
+  }
+  if (time) *time = wall_now() - t0;
+  return true;
+}
+
 bool guarded(const std::function<void()> &fn) {
   try {
     fn();
@@ -798,8 +950,10 @@ void sharp_execute(sharp_jobtype type, int spin, void *alm, void *map,
                    const sharp_geom_info *geom_info, const sharp_alm_info *alm_info, int ntrans,
                    int flags, double *time, unsigned long long *opcnt) {
   sht::guarded([&] {
-    sht::execute_impl(type, spin, alm, map, geom_info, alm_info, ntrans, flags, false, nullptr,
-                      time, opcnt);
+    if (!sht::execute_pipelined(type, spin, alm, map, geom_info, alm_info, ntrans, flags, time,
+                                opcnt))
+      sht::execute_impl(type, spin, alm, map, geom_info, alm_info, ntrans, flags, false, nullptr,
+                        time, opcnt);
   });
 }
 
