@@ -473,8 +473,19 @@ mixed_synth_kernel(const int2 *__restrict__ items, const int *__restrict__ count
         break;
       }
       unsigned char *at = sA + (sa * kRS + rs) * S::ATILES * kTileBytes;
+      const uint32_t at32 = smem_u32(at);
       uint32_t u[S::T][2][kLP];
       const uint32_t cf = smem_u32(sB + sb * S::BLK);
+      // this thread's row of every A tile, four l of one parity per store,
+      // written as soon as the steps that make them are done
+      auto store4 = [&](int o) {
+#pragma unroll
+        for (int t = 0; t < S::T; ++t)
+#pragma unroll
+          for (int par = 0; par < 2; ++par)
+            sts_u32x4(at32 + (t * 2 + par) * kTileBytes + tile_off(row, 4 * o), u[t][par][o],
+                      u[t][par][o + 1], u[t][par][o + 2], u[t][par][o + 3]);
+      };
 #pragma unroll
       for (int h = 0; h < 2; ++h) {  // two blocks of 16 l-steps
         const bool all = __all_sync(0xffffffffu, act);
@@ -485,6 +496,8 @@ mixed_synth_kernel(const int2 *__restrict__ items, const int *__restrict__ count
           else
             steps16_s0<false>(cf + h * 16 * S::CE, x, act, mu0, mu1, &u[0][0][8 * h],
                               &u[0][1][8 * h]);
+          store4(8 * h);
+          store4(8 * h + 4);
         } else {
 #pragma unroll
           for (int g = 0; g < 2; ++g) {
@@ -496,6 +509,7 @@ mixed_synth_kernel(const int2 *__restrict__ items, const int *__restrict__ count
             else
               steps8_sp<false>(cg, x, act, mu0, mu1, mm0, mm1, &u[0][0][o], &u[S::T - 1][0][o],
                                &u[0][1][o], &u[S::T - 1][1][o]);
+            store4(o);
           }
         }
         // every 16 l-steps: bookkeeping of rings still in the scaled regime
@@ -512,17 +526,6 @@ mixed_synth_kernel(const int2 *__restrict__ items, const int *__restrict__ count
           spin_renorm(live, act, mu0, mu1, mm0, mm1, E, Em);
         }
       }
-      // this thread's row of every A tile: 64 bytes = 4 x 16
-      const uint32_t at32 = smem_u32(at);
-#pragma unroll
-      for (int t = 0; t < S::T; ++t)
-#pragma unroll
-        for (int par = 0; par < 2; ++par)
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            sts_u32x4(at32 + (t * 2 + par) * kTileBytes + tile_off(row, 16 * q),
-                      u[t][par][4 * q], u[t][par][4 * q + 1], u[t][par][4 * q + 2],
-                      u[t][par][4 * q + 3]);
       fence_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&full_a[sa]);
