@@ -63,6 +63,7 @@ void dev_free(T *&p) {
 std::vector<int> factor_fft(int N) {
   std::vector<int> r;
   int n = N;
+  while (n % 8 == 0) { r.push_back(8); n /= 8; }
   while (n % 4 == 0) { r.push_back(4); n /= 4; }
   while (n % 2 == 0) { r.push_back(2); n /= 2; }
   for (int p = 3; n > 1; p += 2)
@@ -168,7 +169,7 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
         // Stockham cost ~ N * sum(generic radices); Bluestein ~ M log2 M + 2N
         // (power-of-two convolution of length M >= 2N-1)
         long long direct = 0;
-        for (int r : rad) direct += (r > 5) ? r : 1;
+        for (int r : rad) direct += (r > 5 && r != 8) ? r : 1;
         direct *= d.N;
         int M = 1, lg = 0;
         while (M < 2 * d.N - 1) { M <<= 1; ++lg; }

@@ -78,6 +78,7 @@ constexpr double kC5b = -0.80901699437494742410;  // cos(4 pi/5)
 constexpr double kS5a = 0.95105651629515357212;   // sin(2 pi/5)
 constexpr double kS5b = 0.58778525229247312917;   // sin(4 pi/5)
 constexpr double kS3 = 0.86602540378443864676;    // sin(2 pi/3)
+constexpr double kR2 = 0.70710678118654752440;    // cos(pi/4)
 
 __device__ __forceinline__ double2 mul_i(double2 a) { return make_double2(-a.y, a.x); }
 
@@ -102,6 +103,26 @@ __device__ __forceinline__ void small_dft(double2 (&v)[R], bool inv) {
     v[0] = cadd(v[0], t);
     v[1] = cadd(u, d);
     v[2] = csub(u, d);
+  } else if constexpr (R == 8) {
+    // 8 = 2 x 4: DFT-2 over n1 of x[4 n1 + n2], twiddles w8^n2 on the odd
+    // outputs, DFT-4 over n2; output X[k1 + 2 k2]
+    double2 a0[4], a1[4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      a0[n2] = cadd(v[n2], v[n2 + 4]);
+      a1[n2] = csub(v[n2], v[n2 + 4]);
+    }
+    const double sg = inv ? 1.0 : -1.0;   // w8^e = (cos(e pi/4), sg sin(e pi/4))
+    a1[1] = cmul(a1[1], make_double2(kR2, sg * kR2));
+    a1[2] = make_double2(-sg * a1[2].y, sg * a1[2].x);     // times (0, sg)
+    a1[3] = cmul(a1[3], make_double2(-kR2, sg * kR2));
+    small_dft<4>(a0, inv);
+    small_dft<4>(a1, inv);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+      v[2 * k2] = a0[k2];
+      v[2 * k2 + 1] = a1[k2];
+    }
   } else if constexpr (R == 5) {
     const double2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
     const double2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
@@ -190,6 +211,7 @@ __device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv, 
       case 3: stockham_small<3>(src, dst, d.N, Ns, inv, W, step); break;
       case 4: stockham_small<4>(src, dst, d.N, Ns, inv, W, step); break;
       case 5: stockham_small<5>(src, dst, d.N, Ns, inv, W, step); break;
+      case 8: stockham_small<8>(src, dst, d.N, Ns, inv, W, step); break;
       default: stockham_generic(src, dst, d.N, R, Ns, inv, W, step); break;
     }
     __syncthreads();
