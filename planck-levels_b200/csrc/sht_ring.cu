@@ -10,7 +10,7 @@
 // One CTA owns one (ring pair, component) and runs both hemispheres.  The FFT
 // is a Stockham auto-sort mixed-radix transform in shared memory: even ring
 // lengths n use a complex FFT of length n/2 on packed (x_2j + i x_2j+1) data;
-// odd lengths a complex FFT of length n.  Radix-2/3/4/5 stages and a generic
+// odd lengths a complex FFT of length n.  Radix-2/3/4/5/8 stages and a generic
 // prime stage share one code path (each thread computes whole outputs, so
 // large prime factors parallelise over outputs).  Twiddles come from a
 // per-length table exp(-2 pi i j/n) computed once per geometry; each ring
