@@ -18,12 +18,12 @@
 //    group's maximum; row (hc, w) holds class w of (half, column) hc.  Built
 //    once per group, it stays in TMEM while the group sweeps all l, so the
 //    MMAs read only the B operand from shared memory.
-//  * B (shared memory, N = 64 consecutive l, K as A): the words
+//  * B (shared memory, N = 80 consecutive l, K as A): the words
 //    u_l(p) = 2^31 + round(lambda_l(p) 2^30 / b_l) with the analytic bound
 //    b_l (sqrt((2l+1)/4pi) at spin 0; 1 for each of d^l_{m,+-s}), one
 //    magic-constant DFMA each; a producer thread owns one ring pair and
 //    writes one (spin: two) 4-byte words per l.
-//  * D (int32, TMEM, 128 lanes x 64 columns per l-tile, two buffers): the
+//  * D (int32, TMEM, 128 lanes x 80 columns per l-tile, two buffers): the
 //    exact class sums over the group's ring pairs.  A tile is read back
 //    through shared memory, its five class sums per (l, half, column)
 //    combined exactly in 64-bit integers, corrected for the 2^31 offset and
@@ -52,13 +52,14 @@ namespace sht {
 
 namespace {
 
-constexpr int kAM = 64;                       // l per tile (MMA N)
+constexpr int kAM = 80;                       // l per tile (MMA N; a multiple of 16)
 constexpr int kAClasses = 5;                  // byte-product weights 2^16 .. 2^48
 constexpr int kHCW = 6;                       // (half, column) groups per TMEM subpartition
-// B slice of one producer warp and tile (64 l x the warp's ring pairs,
+// B slice of one producer warp and tile (kAM l x the warp's ring pairs,
 // K-major, no swizzle): the 8-row groups are contiguous (SBO = 128) and the K
-// core matrices lie kALBO = 8*128 + 16 bytes apart, so the per-l stores of a
-// warp spread over all 32 banks.
+// core matrices lie kALBO = (kAM/8)*128 + 16 bytes apart, so the per-l stores
+// of a warp spread over all 32 banks.  An MMA of N = 80 costs about what one
+// of N = 64 does (the issue floor), so 80 l per tile cut the MMA time per l.
 constexpr int kALBO = (kAM / 8) * 128 + 16;
 constexpr int kFRow = 4 * kAM + 16;           // flush staging row (bytes)
 
@@ -90,7 +91,8 @@ struct AShape {
   static constexpr int AROW = KB + 16;                 // A staging row (bytes)
   static constexpr int FLUSH = FW * 32 * kFRow;        // flush staging
   static constexpr int SMEM = STAGES + FLUSH + 2 * COEF;
-  static constexpr uint32_t NCOLS = 512;               // A: 256 columns, D: 2 x 64
+  static constexpr uint32_t NCOLS = 512;               // A: 256 columns, D: 2 x kAM
+  static_assert(ACOLS + 2 * kAM <= 512, "TMEM capacity");
   static_assert(KB == 1024, "K extent of a group");
   static_assert(NH <= 4 * kHCW, "(half, column) groups fit the four subpartitions");
   static_assert(arow(4 * kHCW - 1, kAClasses - 1) * AROW + KB <= STAGES, "A staging");
@@ -241,7 +243,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = tslot;                 // A: columns [0, 256); D: 256 + 64 d
+  const uint32_t tmem = tslot;                 // A: columns [0, 256); D: 256 + kAM d
 
   if (warp == LW) {
     // ------- coefficient loader and MMA issuer (lane 0 issues) -------
@@ -313,7 +315,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
 #pragma unroll
         for (int u = 0; u < kItems; ++u) {
           const int it = ft + u * 32 * FW;
-          const int l = l0 + (it & (kAM - 1));
+          const int l = l0 + (it % kAM);
           const bool v = ok && it < kAM * (S::NCOL / 2) && l <= lmax;
           po[u] = v ? Aout[(mo + l) * ncA + comp0 + it / kAM] : make_double2(0.0, 0.0);
           pcq[u] = !v ? 1.0 : S::SPIN ? __ldg(coef + 2 * (mo + l) + 1).x : __ldg(coef + mo + l).y;
@@ -340,7 +342,7 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
 #pragma unroll
           for (int u = 0; u < kItems; ++u) {
             const int it = ft + u * 32 * FW;
-            const int li = it & (kAM - 1), jo = it / kAM;
+            const int li = it % kAM, jo = it / kAM;
             const int l = l0 + li;
             if (it >= kAM * (S::NCOL / 2) || l > lmax) continue;
             double R[4];
