@@ -298,6 +298,28 @@ class Sets:
         return ops
 
 
+def max_over_ranks(dist, torch, value, device):
+    """The largest value over all ranks (the slowest rank's time), or the
+    value itself without a process group."""
+    if not dist:
+        return value
+    tt = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def rank_seed(rank):
+    """Seed of the first input set of a rank: replicas transform distinct
+    inputs."""
+    return 7 + 1000 * rank
+
+
+def whole_job_rate(world, per_rank_units, step_s):
+    """Units processed by all ranks per second when every rank processes
+    per_rank_units in step_s (the max over ranks)."""
+    return world * per_rank_units / step_s
+
+
 def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     """Device time per step (CUDA events on the launching stream, barrier +
     synchronize on both sides), launch count and per-family kernel time."""
@@ -350,10 +372,7 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     lib.sharp_b200_profile(0)
     step_s = evs[0].elapsed_time(evs[-1]) * 1e-3 / steps
     per_step = [round(evs[i].elapsed_time(evs[i + 1]), 2) for i in range(steps)]
-    if dist:
-        tt = torch.tensor([step_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_s = float(tt.item())
+    step_s = max_over_ranks(dist, torch, step_s, "cuda")
     return step_s, launches, fam, per_step
 
 
@@ -392,7 +411,7 @@ def main():
     B = max(1, args.batch) if mixed else 1
     DP = sb.SHARP_DP
     flags = DP | (sb.SHARP_MIXED if mixed else 0)
-    sets = Sets(sb, torch, np, dev, lmax, npix, nalm, B, seed0=7 + 1000 * rank)
+    sets = Sets(sb, torch, np, dev, lmax, npix, nalm, B, seed0=rank_seed(rank))
 
     lib = sb.lib()
     lib.sharp_b200_kernel_launches.restype = C.c_ulonglong
@@ -409,7 +428,7 @@ def main():
         if dist:
             dist.destroy_process_group()
         return
-    value = world * B / step_s
+    value = whole_job_rate(world, B, step_s)
     head_out = [x.clone() for x in sets.m[0] + sets.o[0]]
 
     # the FP64 drop-in on set 0 (ntrans = 1): companion number and the error
@@ -462,10 +481,7 @@ def main():
         host_step()
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
     gc.enable()
-    if dist:
-        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(dist, torch, e2e_s, dev)
     h2d = B * (3 * nalm * 16 + 3 * npix * 8)
     d2h = B * (3 * npix * 8 + 3 * nalm * 16)
     t_in = sets.host[0][0]
@@ -497,7 +513,7 @@ def main():
                             "kernel_ms_per_step": {k: round(v[0] / (args.fp64_steps if mixed
                                                                       else args.steps), 3)
                                                    for k, v in fp64_fam.items()}},
-            "e2e": {"value": world * B / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e": {"value": whole_job_rate(world, B, e2e_s), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "host_buffers": "distinct" if nh == B else "shared"},
             "gpu_launches": int(launches),
             "roofline": roof,
