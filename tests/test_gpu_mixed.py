@@ -249,3 +249,49 @@ def test_mixed_nside4096_lmax8192_round_trip():
         for x, y in zip(amx, a64):
             assert (torch.linalg.norm(x - y) / torch.linalg.norm(y)).item() < TOL
         del alms, m64, mmx, a64, amx
+
+
+@pytest.mark.parametrize("jtype,spin,flags", [
+    (sb.SHARP_ALM2MAP, 2, DP | MIXED), (sb.SHARP_MAP2ALM, 2, DP | MIXED),
+    (sb.SHARP_ALM2MAP, 0, DP), (sb.SHARP_MAP2ALM, 0, DP | MIXED)])
+def test_host_arrays_in_pieces_equal_device_call(jtype, spin, flags):
+    # a host-array job of several transforms runs in pieces with overlapped
+    # copies (pinned buffers here); its outputs must equal those of one
+    # device-pointer call on the same inputs, bit for bit
+    import torch
+    nside, lmax, nt = 32, 64, 7
+    g, a = sb.Geometry.healpix(nside), sb.AlmInfo.triangular(lmax)
+    nc = 1 if spin == 0 else 2
+    npix, nalm = 12 * nside * nside, sb.nalm_triangular(lmax)
+    rng = np.random.default_rng(spin + 10 * jtype)
+
+    def pinned(n, dtype):
+        return torch.empty(n, dtype=dtype, pin_memory=True).numpy()
+
+    if jtype == sb.SHARP_ALM2MAP:
+        ins = [pinned(nalm, torch.complex128) for _ in range(nt * nc)]
+        for i, x in enumerate(ins):
+            x[:] = uniform_alm(lmax, seed=90 + i, spin=spin)
+        outs = [pinned(npix, torch.float64) for _ in range(nt * nc)]
+        for x in outs:
+            x[:] = 0.0
+        sb.execute(jtype, spin, ins, outs, g, a, nt, flags)
+        d_in = [torch.view_as_real(torch.from_numpy(x.copy()).cuda()).reshape(-1) for x in ins]
+        d_out = [torch.zeros(npix, dtype=torch.float64, device="cuda") for _ in outs]
+        sb.execute_device(jtype, spin, d_in, d_out, g, a, nt, flags)
+    else:
+        ins = [pinned(npix, torch.float64) for _ in range(nt * nc)]
+        for x in ins:
+            x[:] = rng.standard_normal(npix)
+        outs = [pinned(nalm, torch.complex128) for _ in range(nt * nc)]
+        for x in outs:
+            x[:] = 0.0
+        sb.execute(jtype, spin, outs, ins, g, a, nt, flags)
+        d_in = [torch.from_numpy(x.copy()).cuda() for x in ins]
+        d_out = [torch.zeros(2 * nalm, dtype=torch.float64, device="cuda") for _ in outs]
+        sb.execute_device(jtype, spin, d_out, d_in, g, a, nt, flags)
+    torch.cuda.synchronize()
+    for h, d in zip(outs, d_out):
+        got = d.cpu().numpy()
+        want = h.view(np.float64) if h.dtype == np.complex128 else h
+        assert np.array_equal(got, want)
