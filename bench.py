@@ -352,9 +352,12 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     # process: run it here and keep the collector off while timing
     gc.collect()
     gc.disable()
+    host = []
     evs[0].record(stream)
     for i in range(steps):
+        h0 = time.perf_counter()
         fn()
+        host.append(round((time.perf_counter() - h0) * 1e3, 2))
         evs[i + 1].record(stream)
     torch.cuda.synchronize()
     gc.enable()
@@ -373,7 +376,10 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     step_s = evs[0].elapsed_time(evs[-1]) * 1e-3 / steps
     per_step = [round(evs[i].elapsed_time(evs[i + 1]), 2) for i in range(steps)]
     step_s = max_over_ranks(dist, torch, step_s, "cuda")
-    return step_s, launches, fam, per_step
+    # per_step: device time between the step events; host: time the host
+    # took to enqueue each step (a step whose device time exceeds its kernels'
+    # sum by more than its host time waited on something outside the library)
+    return step_s, launches, fam, {"device": per_step, "host_enqueue": host}
 
 
 def rel(torch, a, b):
@@ -519,7 +525,8 @@ def main():
             "roofline": roof,
             "kernel_time_share": share,
             "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in fam.items()},
-            "step_ms": per_step,
+            "step_ms": per_step["device"],
+            "step_host_enqueue_ms": per_step["host_enqueue"],
             "clocks": clk.summary(),
             "check": {"round_trip_rel_err_no_iteration": rt_err, "device_vs_host_api": api_err}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -194,4 +194,17 @@ class ProfScope {
 void check_cuda(cudaError_t e, const char *what, const char *file, int line);
 #define SHT_CUDA(call) ::sht::check_cuda((call), #call, __FILE__, __LINE__)
 
+// Stream-ordered workspace allocation from the library's own memory pool on
+// the current device (free with cudaFreeAsync).  The pool keeps freed memory
+// mapped across synchronizes (release threshold unlimited): with the
+// device's default pool every synchronize returned the workspace to the
+// driver and the next transform mapped several GB again before its first
+// kernel.  ws_trim() hands the unused memory back (sharp_b200_release_cache).
+cudaError_t ws_alloc_bytes(void **p, size_t bytes, cudaStream_t st);
+template <typename T>
+inline cudaError_t ws_alloc(T **p, size_t bytes, cudaStream_t st) {
+  return ws_alloc_bytes(reinterpret_cast<void **>(p), bytes, st);
+}
+void ws_trim();
+
 }  // namespace sht

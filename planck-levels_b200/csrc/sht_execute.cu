@@ -95,6 +95,49 @@ std::map<const void *, std::vector<std::unique_ptr<GeomPlan>>> g_geom_cache;
 std::vector<std::unique_ptr<CoefPlan>> g_coef_cache;
 std::map<const void *, std::unique_ptr<AlmPlan>> g_alm_cache;
 
+}  // namespace
+
+// workspace pools, one per device, created on first use
+static std::mutex g_pool_mutex;
+static std::vector<cudaMemPool_t> g_pools;
+
+cudaError_t ws_alloc_bytes(void **p, size_t bytes, cudaStream_t st) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mutex);
+    if (int(g_pools.size()) <= dev) g_pools.resize(dev + 1, nullptr);
+    if (!g_pools[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaMemPool_t created = nullptr;
+      e = cudaMemPoolCreate(&created, &props);
+      if (e != cudaSuccess) return e;
+      uint64_t keep = UINT64_MAX;
+      e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) {
+        cudaMemPoolDestroy(created);
+        return e;
+      }
+      g_pools[dev] = created;
+    }
+    pool = g_pools[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+void ws_trim() {
+  std::lock_guard<std::mutex> lk(g_pool_mutex);
+  for (cudaMemPool_t pool : g_pools)
+    if (pool) cudaMemPoolTrimTo(pool, 0);
+}
+
+namespace {
+
 // ---------------------------------------------------------------------------
 // geometry plan
 // ---------------------------------------------------------------------------
@@ -472,7 +515,7 @@ struct DevBuf {
   cudaStream_t st = nullptr;
   DevBuf() = default;
   DevBuf(size_t bytes, cudaStream_t s) : st(s) {
-    if (bytes) SHT_CUDA(cudaMallocAsync(&p, bytes, s));
+    if (bytes) SHT_CUDA(::sht::ws_alloc(&p, bytes, s));
   }
   ~DevBuf() {
     if (p) cudaFreeAsync(p, st);
@@ -801,8 +844,8 @@ bool execute_pipelined(sharp_jobtype type, int spin, void *alm, void *map,
       // inputs of the piece: host -> device on the input stream
       for (int i = 0; i < nt * ncomp; ++i) {
         const int gi = t0p * ncomp + i;
-        SHT_CUDA(cudaMallocAsync(&pc.dmap[i], esz_map * std::max<long long>(map_n, 1), sin));
-        SHT_CUDA(cudaMallocAsync(&pc.dalm[i], esz_alm * std::max<long long>(alm_n, 1), sin));
+        SHT_CUDA(::sht::ws_alloc(&pc.dmap[i], esz_map * std::max<long long>(map_n, 1), sin));
+        SHT_CUDA(::sht::ws_alloc(&pc.dalm[i], esz_alm * std::max<long long>(alm_n, 1), sin));
         if (load_maps && map_n > 0)
           SHT_CUDA(cudaMemcpyAsync(pc.dmap[i], static_cast<char *>(map_in[gi]) + esz_map * map_lo,
                                    esz_map * map_n, cudaMemcpyHostToDevice, sin));
@@ -988,6 +1031,9 @@ void sharp_b200_release_cache(void) {
   sht::g_geom_cache.clear();
   sht::g_coef_cache.clear();
   sht::g_alm_cache.clear();
+  // workspace freed in stream order is unused once the device is idle
+  cudaDeviceSynchronize();
+  sht::ws_trim();
 }
 
 }  // extern "C"

@@ -569,9 +569,9 @@ void launch_shape(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp, co
   long long *d_ioff = nullptr;
   double *epi = nullptr;
   const size_t epi_bytes = sizeof(double) * 3 * S::NCOL * (mmax + 1);
-  SHT_CUDA(cudaMallocAsync(&img, size_t(tot), st));
-  SHT_CUDA(cudaMallocAsync(&d_ioff, sizeof(long long) * (mmax + 1), st));
-  SHT_CUDA(cudaMallocAsync(&epi, epi_bytes, st));
+  SHT_CUDA(::sht::ws_alloc(&img, size_t(tot), st));
+  SHT_CUDA(::sht::ws_alloc(&d_ioff, sizeof(long long) * (mmax + 1), st));
+  SHT_CUDA(::sht::ws_alloc(&epi, epi_bytes, st));
   SHT_CUDA(cudaMemcpyAsync(d_ioff, ioff.data(), sizeof(long long) * (mmax + 1),
                            cudaMemcpyHostToDevice, st));
   SHT_CUDA(cudaMemsetAsync(img, 0, size_t(tot), st));

@@ -769,8 +769,8 @@ void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
   if (tw_n.empty()) return;
   int *d_n = nullptr, *d_off = nullptr;
   const int nt = int(tw_n.size());
-  SHT_CUDA(cudaMallocAsync(&d_n, sizeof(int) * nt, st));
-  SHT_CUDA(cudaMallocAsync(&d_off, sizeof(int) * nt, st));
+  SHT_CUDA(::sht::ws_alloc(&d_n, sizeof(int) * nt, st));
+  SHT_CUDA(::sht::ws_alloc(&d_off, sizeof(int) * nt, st));
   SHT_CUDA(cudaMemcpyAsync(d_n, tw_n.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, st));
   SHT_CUDA(cudaMemcpyAsync(d_off, tw_off.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, st));
   (void)ntw;
@@ -793,8 +793,8 @@ void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cud
   std::vector<int> pn{gp.P}, po{0};
   {
     int *d_n = nullptr, *d_off = nullptr;
-    SHT_CUDA(cudaMallocAsync(&d_n, sizeof(int), st));
-    SHT_CUDA(cudaMallocAsync(&d_off, sizeof(int), st));
+    SHT_CUDA(::sht::ws_alloc(&d_n, sizeof(int), st));
+    SHT_CUDA(::sht::ws_alloc(&d_off, sizeof(int), st));
     SHT_CUDA(cudaMemcpyAsync(d_n, pn.data(), sizeof(int), cudaMemcpyHostToDevice, st));
     SHT_CUDA(cudaMemcpyAsync(d_off, po.data(), sizeof(int), cudaMemcpyHostToDevice, st));
     ProfScope ps("twiddles", st);
@@ -805,7 +805,7 @@ void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cud
   }
   if (idx.empty()) return;
   int *d_idx = nullptr;
-  SHT_CUDA(cudaMallocAsync(&d_idx, sizeof(int) * idx.size(), st));
+  SHT_CUDA(::sht::ws_alloc(&d_idx, sizeof(int) * idx.size(), st));
   SHT_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st));
   ProfScope ps("bluestein_setup", st);
   bluestein_setup_kernel<<<int(idx.size()), 256, 0, st>>>(gp.fdesc, d_idx, gp.twiddle, gp.wpow2,
@@ -849,7 +849,7 @@ FftLaunch plan_fft_launch(const GeomPlan &gp, int cls, int mmax, int ncomp, cuda
     L.grid = dim3(slots, 1);
     L.thr = 1024;
     L.smem = sizeof(double2) * ring_fft_smem_entries(0, 0, mmax, gp.nmax_complex, gp.P);
-    SHT_CUDA(cudaMallocAsync(&L.gbuf, sizeof(double2) * size_t(slots) *
+    SHT_CUDA(::sht::ws_alloc(&L.gbuf, sizeof(double2) * size_t(slots) *
                                           (gp.cls_bufA[cls] + gp.cls_bufB[cls]), st));
   }
   return L;

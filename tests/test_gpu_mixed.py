@@ -1,5 +1,6 @@
-"""Mixed-precision batched synthesis (SHARP_MIXED): the tcgen05 TF32-split
-contraction against the FP64 engine and the reference.
+"""Mixed-precision batched transforms (SHARP_MIXED): FP64 recurrence, exact
+int8 tcgen05 Legendre contraction, against the FP64 engine and the
+reference.
 
 Tolerance: 1e-6 relative L2 against the FP64 result, the bar stated for the
 mixed-precision form (FP64 recurrence seeds, tensor-core contraction)."""
@@ -295,3 +296,33 @@ def test_host_arrays_in_pieces_equal_device_call(jtype, spin, flags):
         got = d.cpu().numpy()
         want = h.view(np.float64) if h.dtype == np.complex128 else h
         assert np.array_equal(got, want)
+
+
+def test_workspace_stays_mapped_until_release_cache():
+    # workspace comes from the library's own pool, which keeps it mapped
+    # across synchronizes (a transform after a synchronize does not map it
+    # again); sharp_b200_release_cache() hands it back to the driver.  The
+    # results do not depend on whether the workspace was reused.
+    import torch
+    nside, lmax, nt = 512, 1024, 8
+    g, a = sb.Geometry.healpix(nside), sb.AlmInfo.triangular(lmax)
+    alms = [uniform_alm(lmax, seed=200 + i) for i in range(nt)]
+
+    def run():
+        maps = [np.zeros(12 * nside * nside) for _ in range(nt)]
+        sb.execute(sb.SHARP_ALM2MAP, 0, [x.copy() for x in alms], maps, g, a, nt, DP | MIXED)
+        return maps
+
+    torch.cuda.synchronize()
+    sb.lib().sharp_b200_release_cache()
+    free0 = torch.cuda.mem_get_info()[0]
+    first = run()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    second = run()                       # reuses the mapped workspace
+    sb.lib().sharp_b200_release_cache()
+    free2 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 > (64 << 20)    # workspace held across the synchronize
+    assert abs(free2 - free0) < (32 << 20)
+    for x, y in zip(first, second):
+        assert np.array_equal(x, y)
