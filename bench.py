@@ -87,12 +87,19 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self.first = 0
+        self.last = None
 
     def mark(self):
-        """Only samples taken after this call enter the summary (the sampler
-        is started before the warm-up: nvidia-smi's start-up stalls the GPU
-        for a moment and must not fall into the timed region)."""
+        """Only samples taken after this call (and before end()) enter the
+        summary.  The sampler runs from the start of the benchmark: the first
+        nvidia-smi on a freshly reset GPU holds the driver for a while, and
+        a workspace allocation waiting on it must not fall into a timed
+        region."""
         self.first = len(self.lines)
+        self.last = None
+
+    def end(self):
+        self.last = len(self.lines)
 
     def __enter__(self):
         try:
@@ -118,7 +125,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines[self.first:]:
+        for ln in self.lines[self.first:self.last]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -323,17 +330,14 @@ def whole_job_rate(world, per_rank_units, step_s):
 def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     """Device time per step (CUDA events on the launching stream, barrier +
     synchronize on both sides), launch count and per-family kernel time."""
-    if clk:
-        clk.__enter__()
-        # nvidia-smi's start-up stalls the GPU for about a second: wait until
-        # it samples (two lines) so the stall stays out of the timed region
-        t_end = time.time() + 15.0
-        while len(clk.lines) < 2 and time.time() < t_end and clk.proc is not None:
-            time.sleep(0.05)
-        time.sleep(0.5)
     lib.sharp_b200_profile(1)   # warm-up runs with the same event instrumentation
-    for _ in range(warmup):
+    for i in range(warmup):
         fn()
+        if i == 0:
+            # the first step after a synchronize grows the library's workspace
+            # pool once (its buffers then no longer fit the chunks the first
+            # step left); let that happen here rather than in the timed steps
+            torch.cuda.synchronize()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -362,7 +366,7 @@ def timed(torch, lib, stream, fn, steps, warmup, dist, clk=None):
     torch.cuda.synchronize()
     gc.enable()
     if clk:
-        clk.__exit__()
+        clk.end()
     if dist:
         dist.barrier()
     launches = lib.sharp_b200_kernel_launches() - l0
@@ -401,6 +405,13 @@ def main():
     import sharp_b200 as sb
 
     torch.cuda.set_device(local)
+    # clocks are sampled from here to the end; the timed regions mark theirs
+    with ClockSampler(local) as clk:
+        run_ours(args, world, rank, local, clk, np, torch, sb)
+
+
+def run_ours(args, world, rank, local, clk, np, torch, sb):
+    """Our arm: timed device steps, the FP64 companion and the e2e run."""
     dist = None
     if world > 1:
         import datetime
@@ -426,7 +437,6 @@ def main():
     stream = torch.cuda.current_stream()
 
     ops = {}
-    clk = ClockSampler(local)
     step_s, launches, fam, per_step = timed(torch, lib, stream,
                                             lambda: sets.step(sb, geom, ainfo, B, flags, ops),
                                             args.steps, args.warmup, dist, clk)
@@ -477,7 +487,10 @@ def main():
         sb.execute(sb.SHARP_MAP2ALM, 2, [x for i in hs for x in h_out[i][1:]],
                    [x for i in hs for x in h_map[i][1:]], geom, ainfo, B, flags)
 
-    host_step()
+    # two untimed steps: every host-array call ends with a synchronize, and
+    # the second such step is where the workspace pool takes its steady size
+    for _ in range(2):
+        host_step()
     if dist:
         dist.barrier()
     gc.collect()

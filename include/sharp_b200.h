@@ -56,6 +56,13 @@ void sharp_b200_forget_geometry (const sharp_geom_info *geom_info);
 /* Frees every cached device table and workspace of the calling process. */
 void sharp_b200_release_cache (void);
 
+/* Device memory of the library's workspace pool on the current device:
+   *reserved = bytes the pool keeps mapped (freed workspace stays mapped for
+   the next job until sharp_b200_release_cache), *used = bytes of live
+   workspace.  Returns 0, or -1 (both set to 0) before the first job on this
+   device.  No counterpart in the reference. */
+int sharp_b200_workspace_bytes (unsigned long long *reserved, unsigned long long *used);
+
 /* Number of CUDA kernels this library has launched in the calling process. */
 unsigned long long sharp_b200_kernel_launches (void);
 

@@ -206,5 +206,6 @@ inline cudaError_t ws_alloc(T **p, size_t bytes, cudaStream_t st) {
   return ws_alloc_bytes(reinterpret_cast<void **>(p), bytes, st);
 }
 void ws_trim();
+bool ws_bytes(unsigned long long *reserved, unsigned long long *used);
 
 }  // namespace sht

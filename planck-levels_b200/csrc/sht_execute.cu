@@ -136,6 +136,20 @@ void ws_trim() {
     if (pool) cudaMemPoolTrimTo(pool, 0);
 }
 
+bool ws_bytes(unsigned long long *reserved, unsigned long long *used) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  std::lock_guard<std::mutex> lk(g_pool_mutex);
+  if (int(g_pools.size()) <= dev || !g_pools[dev]) return false;
+  uint64_t r = 0, u = 0;
+  if (cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrReservedMemCurrent, &r) != cudaSuccess ||
+      cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrUsedMemCurrent, &u) != cudaSuccess)
+    return false;
+  if (reserved) *reserved = r;
+  if (used) *used = u;
+  return true;
+}
+
 namespace {
 
 // ---------------------------------------------------------------------------
@@ -449,22 +463,6 @@ AlmPlan *get_alm_plan(const sharp_alm_info *a, int mmax, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // per-device library stream
 // ---------------------------------------------------------------------------
-// Keeps freed workspace in the device's default pool instead of returning it
-// to the driver at every synchronisation (re-mapping gigabytes of workspace
-// per call costs tens of milliseconds).  Once per device.
-void retain_pool_memory() {
-  static std::set<int> done;
-  int dev = 0;
-  SHT_CUDA(cudaGetDevice(&dev));
-  if (done.count(dev)) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t thr = ~0ull;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
-  done.insert(dev);
-}
-
 cudaStream_t library_stream() {
   static std::map<int, cudaStream_t> streams;
   int dev = 0;
@@ -595,7 +593,6 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
     }
 
   std::lock_guard<std::mutex> lk(g_cache_mutex);
-  retain_pool_memory();
   if (flags & SHARP_MIXED) check_tc_error();
   cudaStream_t st = device_ptrs ? user_stream : library_stream();
   GeomPlan *gp = get_geom_plan(ginfo, job.lmax, mmax, spin, st);
@@ -801,7 +798,6 @@ bool execute_pipelined(sharp_jobtype type, int spin, void *alm, void *map,
   cudaStream_t cs = library_stream();
   {
     std::lock_guard<std::mutex> lk(g_cache_mutex);
-    retain_pool_memory();
     const int mmax = ainfo->nm - 1;
     GeomPlan *gp = get_geom_plan(ginfo, ainfo->lmax, mmax, spin, cs);
     AlmPlan *ap = get_alm_plan(ainfo, mmax, cs);
@@ -1034,6 +1030,12 @@ void sharp_b200_release_cache(void) {
   // workspace freed in stream order is unused once the device is idle
   cudaDeviceSynchronize();
   sht::ws_trim();
+}
+
+int sharp_b200_workspace_bytes(unsigned long long *reserved, unsigned long long *used) {
+  if (reserved) *reserved = 0;
+  if (used) *used = 0;
+  return sht::ws_bytes(reserved, used) ? 0 : -1;
 }
 
 }  // extern "C"

@@ -661,7 +661,8 @@ void launch_mixed_anal(const JobDesc &job, const GeomPlan &gp, CoefPlan &cp,
   if (!cp.mx_coef) {
     // a tile's coefficients are copied whole: kAM entries of slack at the end
     const size_t n = (size_t(cp.total) + kAM) * (cp.spin == 0 ? 1 : 2);
-    SHT_CUDA(::sht::ws_alloc(&cp.mx_coef, sizeof(double2) * n, st));
+    // a table of the plan (freed with it by cudaFree), not workspace
+    SHT_CUDA(cudaMalloc(&cp.mx_coef, sizeof(double2) * n));
     SHT_CUDA(cudaMemsetAsync(cp.mx_coef, 0, sizeof(double2) * n, st));
     mixed_anal_coef_kernel<<<cp.mmax + 1, 256, 0, st>>>(cp.lmax, cp.mmax, cp.spin, cp.d_moff,
                                                         cp.alpha, cp.beta, cp.cfac, cp.mx_coef);

@@ -96,6 +96,19 @@ def lib():
     return _lib
 
 
+_lib.sharp_b200_workspace_bytes.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]
+_lib.sharp_b200_workspace_bytes.restype = C.c_int
+
+
+def workspace_bytes():
+    """(reserved, used) bytes of the library's workspace pool on the current
+    device: freed workspace stays reserved for the next job until
+    sharp_b200_release_cache().  (0, 0) before the first job."""
+    r, u = C.c_ulonglong(0), C.c_ulonglong(0)
+    _lib.sharp_b200_workspace_bytes(C.byref(r), C.byref(u))
+    return r.value, u.value
+
+
 def last_error() -> str:
     return _lib.sharp_b200_last_error().decode()
 
