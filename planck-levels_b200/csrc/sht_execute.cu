@@ -297,6 +297,9 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
             bufA = std::max(bufA, d.blue ? std::max(d.M, d.N + 2) : d.N + 2);
             bufB = std::max(bufB, d.N + 2);
           }
+      // whole blocks of 8 entries: the ring kernels swizzle indices inside them
+      bufA = (bufA + 7) & ~7;
+      bufB = (bufB + 7) & ~7;
       gp->cls_N.push_back(std::max(bounds[c], 1));
       gp->cls_bufA.push_back(bufA);
       gp->cls_bufB.push_back(bufB);

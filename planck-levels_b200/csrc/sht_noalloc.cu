@@ -192,6 +192,8 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
           nmaxc = std::max(nmaxc, d.N);
         }
     cls_N.push_back(std::min(bounds[c], std::max(nmaxc, 1)));
+    bufA = (bufA + 7) & ~7;   // whole blocks of 8 (swizzled in the ring kernels)
+    bufB = (bufB + 7) & ~7;
     cls_bufA.push_back(bufA);
     cls_bufB.push_back(bufB);
     cls_start.push_back(int(flat.size()));

@@ -44,6 +44,17 @@ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -
 __device__ __forceinline__ double2 cscale(double2 a, double s) {
   return make_double2(a.x * s, a.y * s);
 }
+// FFT buffer (shared memory, or a CTA's slot of global scratch) whose element
+// index is swizzled inside aligned blocks of 8 entries (16-byte units):
+// e -> e ^ ((e >> 3) & 7).  The butterflies' strided stores (2, 4 or 8
+// entries apart) and contiguous runs then spread over the bank groups of a
+// 128-byte wavefront.  The map permutes each block, so a buffer of a
+// multiple of 8 entries holds the indices [0, size); elementwise work on
+// two buffers stored the same way may index them directly.
+struct Buf {
+  double2 *p;
+  __device__ __forceinline__ double2 &operator[](int e) const { return p[e ^ ((e >> 3) & 7)]; }
+};
 
 // exp(-2 pi i e/n), 0 <= e < n, read from the per-length global table
 struct TwGlobal {
@@ -141,7 +152,7 @@ __device__ __forceinline__ void small_dft(double2 (&v)[R], bool inv) {
 }
 
 template <int R, class TW>
-__device__ void stockham_small(const double2 *src, double2 *dst, int N, int Ns, bool inv,
+__device__ void stockham_small(Buf src, Buf dst, int N, int Ns, bool inv,
                                const TW &tw, int step) {
   const int NR = N / R;
   const int sf = N / (Ns * R);
@@ -172,7 +183,7 @@ __device__ void stockham_small(const double2 *src, double2 *dst, int N, int Ns, 
 // Generic prime radix: each thread computes whole outputs (parallel over
 // the N outputs, so a large prime factor does not serialise a few threads).
 template <class TW>
-__device__ void stockham_generic(const double2 *src, double2 *dst, int N, int R, int Ns,
+__device__ void stockham_generic(Buf src, Buf dst, int N, int R, int Ns,
                                  bool inv, const TW &tw, int step) {
   const int NR = N / R;
   const int sf = N / (Ns * R);
@@ -203,16 +214,16 @@ template <class TW>
 __device__ double2 *run_fft(const FftDesc &d, double2 *a, double2 *b, bool inv, const TW &W) {
   const int step = d.n / d.N;
   int Ns = 1;
-  double2 *src = a, *dst = b;
+  double2 *src = a, *dst = b;   // raw; each pass indexes them through Buf
   for (int s = 0; s < d.nrad; ++s) {
     const int R = d.rad[s];
     switch (R) {
-      case 2: stockham_small<2>(src, dst, d.N, Ns, inv, W, step); break;
-      case 3: stockham_small<3>(src, dst, d.N, Ns, inv, W, step); break;
-      case 4: stockham_small<4>(src, dst, d.N, Ns, inv, W, step); break;
-      case 5: stockham_small<5>(src, dst, d.N, Ns, inv, W, step); break;
-      case 8: stockham_small<8>(src, dst, d.N, Ns, inv, W, step); break;
-      default: stockham_generic(src, dst, d.N, R, Ns, inv, W, step); break;
+      case 2: stockham_small<2>(Buf{src}, Buf{dst}, d.N, Ns, inv, W, step); break;
+      case 3: stockham_small<3>(Buf{src}, Buf{dst}, d.N, Ns, inv, W, step); break;
+      case 4: stockham_small<4>(Buf{src}, Buf{dst}, d.N, Ns, inv, W, step); break;
+      case 5: stockham_small<5>(Buf{src}, Buf{dst}, d.N, Ns, inv, W, step); break;
+      case 8: stockham_small<8>(Buf{src}, Buf{dst}, d.N, Ns, inv, W, step); break;
+      default: stockham_generic(Buf{src}, Buf{dst}, d.N, R, Ns, inv, W, step); break;
     }
     __syncthreads();
     Ns *= R;
@@ -246,7 +257,8 @@ __device__ __forceinline__ double2 chirp_of(int j, int n, int N, const TW &Wn) {
 // stages.  A stage of length len maps x_{i + j len/4} (j < 4) to
 // y_r = W_len^{ir} sum_j x_{i + j len/4} (-i)^{jr}, stored at i + r len/4.
 template <class TW>
-__device__ void dif_inplace(double2 *a, int M, const TW &Wp, int P) {
+__device__ void dif_inplace(double2 *buf, int M, const TW &Wp, int P) {
+  const Buf a{buf};
   const int lg = 31 - __clz(M);
   int len = M;
   if (lg & 1) {
@@ -280,7 +292,8 @@ __device__ void dif_inplace(double2 *a, int M, const TW &Wp, int P) {
 // Inverse of dif_inplace (conjugate twiddles, unnormalised): the stages in
 // reverse order, each mapping its digit order back to natural order.
 template <class TW>
-__device__ void dit_inplace_inv(double2 *a, int M, const TW &Wp, int P) {
+__device__ void dit_inplace_inv(double2 *buf, int M, const TW &Wp, int P) {
+  const Buf a{buf};
   const int lg = 31 - __clz(M);
   const int top = (lg & 1) ? (M >> 1) : M;
   for (int len = 4; len <= top; len <<= 2) {
@@ -315,9 +328,10 @@ __device__ void dit_inplace_inv(double2 *a, int M, const TW &Wp, int P) {
 
 // Input x in buf[0, N); buf holds M entries.  Result in buf[0, N).
 template <class TW>
-__device__ void run_bluestein(const FftDesc &d, double2 *buf, bool inv, const TW &Wn,
+__device__ void run_bluestein(const FftDesc &d, double2 *raw, bool inv, const TW &Wn,
                               const TW &wpow2, int P, const double2 *__restrict__ bhat) {
-  const double2 *bh = bhat + d.bhat;
+  const double2 *bh = bhat + d.bhat;   // stored with the same swizzle as buf
+  const Buf buf{raw};
   for (int j = threadIdx.x; j < d.M; j += blockDim.x) {
     if (j < d.N) {
       double2 x = buf[j];
@@ -328,10 +342,10 @@ __device__ void run_bluestein(const FftDesc &d, double2 *buf, bool inv, const TW
     }
   }
   __syncthreads();
-  dif_inplace(buf, d.M, wpow2, P);
-  for (int k = threadIdx.x; k < d.M; k += blockDim.x) buf[k] = cmul(buf[k], __ldg(bh + k));
+  dif_inplace(raw, d.M, wpow2, P);
+  for (int k = threadIdx.x; k < d.M; k += blockDim.x) raw[k] = cmul(raw[k], __ldg(bh + k));
   __syncthreads();
-  dit_inplace_inv(buf, d.M, wpow2, P);
+  dit_inplace_inv(raw, d.M, wpow2, P);
   for (int k = threadIdx.x; k < d.N; k += blockDim.x) {
     double2 y = cmul(buf[k], chirp_of(k, d.n, d.N, Wn));
     if (inv) y.y = -y.y;
@@ -348,13 +362,13 @@ __global__ void bluestein_setup_kernel(const FftDesc *__restrict__ fdesc,
                                        const double2 *__restrict__ wpow2, int P,
                                        double2 *__restrict__ bhat) {
   const FftDesc d = fdesc[blue_idx[blockIdx.x]];
-  double2 *b = bhat + d.bhat;
+  double2 *b = bhat + d.bhat;    // M (a power of two >= 64) entries, swizzled as Buf
   const TwGlobal Wn{twiddle + d.tw};
   for (int j = threadIdx.x; j < d.M; j += blockDim.x) {
     int jj = -1;
     if (j < d.N) jj = j;
     else if (j > d.M - d.N) jj = d.M - j;
-    b[j] = (jj >= 0) ? cconj(chirp_of(jj, d.n, d.N, Wn)) : make_double2(0.0, 0.0);
+    Buf{b}[j] = (jj >= 0) ? cconj(chirp_of(jj, d.n, d.N, Wn)) : make_double2(0.0, 0.0);
   }
   __syncthreads();
   dif_inplace(b, d.M, TwGlobal{wpow2}, P);
@@ -438,7 +452,7 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
     const double ph = phi0[ring];
     const bool rot = fabs(ph) >= 1e-14;
     const int half = n / 2;  // highest bin kept (n odd: (n-1)/2)
-    double2 *C = bufB;
+    const Buf C{bufB}, Ab{bufA};
     const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
     if (rot) build_shift(slo, shi, mm, ph);
     load_twshared(twlo, twhi, twiddle + d.tw, n);
@@ -467,11 +481,11 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
         const double2 sm = cadd(ck, cn), df = csub(ck, cn);
         const double2 w = tw(k);                    // exp(-2 pi i k/n)
         const double2 iw = make_double2(w.y, w.x);  // i * conj(w)
-        bufA[k] = cadd(sm, cmul(iw, df));
+        Ab[k] = cadd(sm, cmul(iw, df));
       }
     } else {
       for (int k = threadIdx.x; k < n; k += blockDim.x)
-        bufA[k] = (k <= half) ? C[k] : cconj(C[n - k]);
+        Ab[k] = (k <= half) ? C[k] : cconj(C[n - k]);
     }
     __syncthreads();
     double2 *res;
@@ -483,14 +497,15 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
     }
     const long long o = ofs[ring] - map_lo;
     const long long st = stride[ring];
+    const Buf Rs{res};
     if ((n & 1) == 0) {
       for (int j = threadIdx.x; j < d.N; j += blockDim.x) {
-        const double2 z = res[j];
+        const double2 z = Rs[j];
         store_px(map + o + (2 * j) * st, z.x, add);
         store_px(map + o + (2 * j + 1) * st, z.y, add);
       }
     } else {
-      for (int j = threadIdx.x; j < n; j += blockDim.x) store_px(map + o + j * st, res[j].x, add);
+      for (int j = threadIdx.x; j < n; j += blockDim.x) store_px(map + o + j * st, Rs[j].x, add);
     }
     __syncthreads();
   }
@@ -545,12 +560,13 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
     const long long st = stride[ring];
     if (rot) build_shift(slo, shi, mm, -ph);
     load_twshared(twlo, twhi, twiddle + d.tw, n);
+    const Buf Ab{bufA};
     if ((n & 1) == 0) {
       for (int j = threadIdx.x; j < d.N; j += blockDim.x)
-        bufA[j] = make_double2(double(map[o + (2 * j) * st]), double(map[o + (2 * j + 1) * st]));
+        Ab[j] = make_double2(double(map[o + (2 * j) * st]), double(map[o + (2 * j + 1) * st]));
     } else {
       for (int j = threadIdx.x; j < n; j += blockDim.x)
-        bufA[j] = make_double2(double(map[o + j * st]), 0.0);
+        Ab[j] = make_double2(double(map[o + j * st]), 0.0);
     }
     __syncthreads();
     double2 *res;
@@ -560,12 +576,12 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
     } else {
       res = run_fft(d, bufA, bufB, false, tw);
     }
-    double2 *X = (res == bufA) ? bufB : bufA;
+    const Buf X{(res == bufA) ? bufB : bufA}, Rs{res};
     if ((n & 1) == 0) {
       // X_k = (Z_k + conj Z_{N-k})/2 - i W^k (Z_k - conj Z_{N-k})/2, k <= N
       for (int k = threadIdx.x; k <= d.N; k += blockDim.x) {
-        const double2 zk = res[k == d.N ? 0 : k];
-        const double2 zn = cconj(res[k == 0 ? 0 : d.N - k]);
+        const double2 zk = Rs[k == d.N ? 0 : k];
+        const double2 zn = cconj(Rs[k == 0 ? 0 : d.N - k]);
         const double2 sm = cadd(zk, zn), df = csub(zk, zn);
         const double2 w = tw(k);
         const double2 mi_w = make_double2(w.y, -w.x);  // -i * w
@@ -575,7 +591,7 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
       }
     } else {
       for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        double2 xk = res[k];
+        double2 xk = Rs[k];
         if (k == 0) xk.y = 0.0;
         X[k] = xk;
       }
