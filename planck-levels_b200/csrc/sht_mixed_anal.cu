@@ -155,7 +155,8 @@ __host__ __device__ constexpr uint32_t make_idesc_s8u8(int m, int n) {
 }
 
 // Per-m coefficient table of the analysis, for l = m .. lmax + kPad:
-// spin 0: (alpha_l, c_l 2^30 / b_l); spin s: (a_l, b_l), (c_l 2^30, 0).
+// spin 0: (alpha_l, c_l 2^30 / b_l); spin s: (a_l, b_l), (c_l 2^30, 1 / c_l)
+// (the second entry of the spin record is the flush's row factor).
 __global__ void mixed_anal_coef_kernel(int lmax, int mmax, int spin,
                                        const long long *__restrict__ moff,
                                        const double *__restrict__ ca,
@@ -173,7 +174,8 @@ __global__ void mixed_anal_coef_kernel(int lmax, int mmax, int spin,
       out[base + i] = make_double2(ca[base + i], cfac[base + i] * kQ / b);
     } else {
       out[2 * (base + i)] = make_double2(ca[base + i], cb[base + i]);
-      out[2 * (base + i) + 1] = make_double2(cfac[base + i] * kQ, 0.0);
+      const double c = cfac[base + i];
+      out[2 * (base + i) + 1] = make_double2(c * kQ, c != 0.0 ? 1.0 / c : 0.0);
     }
   }
 }
@@ -318,7 +320,8 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
           const int l = l0 + (it % kAM);
           const bool v = ok && it < kAM * (S::NCOL / 2) && l <= lmax;
           po[u] = v ? Aout[(mo + l) * ncA + comp0 + it / kAM] : make_double2(0.0, 0.0);
-          pcq[u] = !v ? 1.0 : S::SPIN ? __ldg(coef + 2 * (mo + l) + 1).x : __ldg(coef + mo + l).y;
+          // spin s: the row factor 1 / c_l itself; spin 0: c_l 2^30 / b_l
+          pcq[u] = !v ? 1.0 : S::SPIN ? __ldg(coef + 2 * (mo + l) + 1).y : __ldg(coef + mo + l).y;
         }
         if (ok) ok = __all_sync(0xffffffffu, mbar_wait(&dfull[d], (J >> 1) & 1));
         // staging of the previous tile is no longer read
@@ -357,8 +360,9 @@ mixed_anal_kernel(const int *__restrict__ count, const double *__restrict__ cth,
               const double Pd = __longlong_as_double(P + 0x4338000000000000LL) - 6755399441055744.0;
               R[e] = (fma(i2d_exact(c[4]), 4294967296.0, Pd) - fco[hc]) * fsc[hc];
             }
-            // lambda was quantised as c_l mu_l 2^30 / b_l: row factor b_l / c_l = 2^30 / cq_l
-            const double b = kQ / pcq[u];
+            // lambda was quantised as c_l mu_l 2^30 / b_l: row factor
+            // b_l / c_l = 2^30 / cq_l (spin s: b_l = 1, read from the table)
+            const double b = S::SPIN ? pcq[u] : kQ / pcq[u];
             const double sg = ((l - mhi) & 1) ? -b : b;
             double2 o = po[u];
             o.x += b * R[0] + sg * R[2];
