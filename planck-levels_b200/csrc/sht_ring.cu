@@ -257,6 +257,46 @@ __device__ __forceinline__ double2 chirp_of(int j, int n, int N, const TW &Wn) {
 // stages.  A stage of length len maps x_{i + j len/4} (j < 4) to
 // y_r = W_len^{ir} sum_j x_{i + j len/4} (-i)^{jr}, stored at i + r len/4.
 template <class TW>
+__device__ __forceinline__ void dif_stage4(const Buf &a, int M, int len, const TW &Wp, int P) {
+  const int q = len >> 2, st = P / len, lq = 31 - __clz(q);
+  for (int t = threadIdx.x; t < (M >> 2); t += blockDim.x) {
+    const int i = t & (q - 1);
+    const int b0 = (t >> lq) * len + i;
+    const double2 x0 = a[b0], x1 = a[b0 + q], x2 = a[b0 + 2 * q], x3 = a[b0 + 3 * q];
+    const double2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
+    const double2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
+    const double2 md13 = make_double2(d13.y, -d13.x);  // -i (x1 - x3)
+    a[b0] = cadd(s02, s13);
+    a[b0 + q] = cmul(cadd(d02, md13), Wp(i * st));
+    a[b0 + 2 * q] = cmul(csub(s02, s13), Wp(2 * i * st));
+    a[b0 + 3 * q] = cmul(csub(d02, md13), Wp(3 * i * st));
+  }
+  __syncthreads();
+}
+
+// One stage of the inverse (conjugate twiddles), undoing dif_stage4.
+template <class TW>
+__device__ __forceinline__ void dit_stage4(const Buf &a, int M, int len, const TW &Wp, int P) {
+  const int q = len >> 2, st = P / len, lq = 31 - __clz(q);
+  for (int t = threadIdx.x; t < (M >> 2); t += blockDim.x) {
+    const int i = t & (q - 1);
+    const int b0 = (t >> lq) * len + i;
+    const double2 z0 = a[b0];
+    const double2 z1 = cmul(a[b0 + q], cconj(Wp(i * st)));
+    const double2 z2 = cmul(a[b0 + 2 * q], cconj(Wp(2 * i * st)));
+    const double2 z3 = cmul(a[b0 + 3 * q], cconj(Wp(3 * i * st)));
+    const double2 s02 = cadd(z0, z2), d02 = csub(z0, z2);
+    const double2 s13 = cadd(z1, z3), d13 = csub(z1, z3);
+    const double2 pd13 = make_double2(-d13.y, d13.x);  // i (z1 - z3)
+    a[b0] = cadd(s02, s13);
+    a[b0 + q] = cadd(d02, pd13);
+    a[b0 + 2 * q] = csub(s02, s13);
+    a[b0 + 3 * q] = csub(d02, pd13);
+  }
+  __syncthreads();
+}
+
+template <class TW>
 __device__ void dif_inplace(double2 *buf, int M, const TW &Wp, int P) {
   const Buf a{buf};
   const int lg = 31 - __clz(M);
@@ -271,85 +311,106 @@ __device__ void dif_inplace(double2 *buf, int M, const TW &Wp, int P) {
     __syncthreads();
     len = half;
   }
-  for (; len >= 4; len >>= 2) {
-    const int q = len >> 2, st = P / len, lq = 31 - __clz(q);
-    for (int t = threadIdx.x; t < (M >> 2); t += blockDim.x) {
-      const int i = t & (q - 1);
-      const int b0 = (t >> lq) * len + i;
-      const double2 x0 = a[b0], x1 = a[b0 + q], x2 = a[b0 + 2 * q], x3 = a[b0 + 3 * q];
-      const double2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
-      const double2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
-      const double2 md13 = make_double2(d13.y, -d13.x);  // -i (x1 - x3)
-      a[b0] = cadd(s02, s13);
-      a[b0 + q] = cmul(cadd(d02, md13), Wp(i * st));
-      a[b0 + 2 * q] = cmul(csub(s02, s13), Wp(2 * i * st));
-      a[b0 + 3 * q] = cmul(csub(d02, md13), Wp(3 * i * st));
-    }
-    __syncthreads();
-  }
+  for (; len >= 4; len >>= 2) dif_stage4(a, M, len, Wp, P);
 }
 
-// Inverse of dif_inplace (conjugate twiddles, unnormalised): the stages in
-// reverse order, each mapping its digit order back to natural order.
+// Bluestein convolution of x (buf[0, N)) with the chirp: the stages of
+// dif_inplace, the product with the transformed chirp bh (stored in the same
+// digit order and swizzle) and the inverse stages, with three sweeps merged:
+//  * the chirp pre-multiplication into the first DIF stage, whose inputs at
+//    and beyond M/2 >= N are the zero padding;
+//  * the last DIF stage (length 4: unit twiddles), the product and the first
+//    inverse stage, which all act on the same four consecutive entries;
+//  * the last inverse stage into the chirp post-multiplication, of which
+//    only the outputs k < N are needed.
+// The result X_k (k < N) is left in buf[0, N).
 template <class TW>
-__device__ void dit_inplace_inv(double2 *buf, int M, const TW &Wp, int P) {
-  const Buf a{buf};
-  const int lg = 31 - __clz(M);
-  const int top = (lg & 1) ? (M >> 1) : M;
-  for (int len = 4; len <= top; len <<= 2) {
-    const int q = len >> 2, st = P / len, lq = 31 - __clz(q);
-    for (int t = threadIdx.x; t < (M >> 2); t += blockDim.x) {
-      const int i = t & (q - 1);
-      const int b0 = (t >> lq) * len + i;
-      const double2 z0 = a[b0];
-      const double2 z1 = cmul(a[b0 + q], cconj(Wp(i * st)));
-      const double2 z2 = cmul(a[b0 + 2 * q], cconj(Wp(2 * i * st)));
-      const double2 z3 = cmul(a[b0 + 3 * q], cconj(Wp(3 * i * st)));
-      const double2 s02 = cadd(z0, z2), d02 = csub(z0, z2);
-      const double2 s13 = cadd(z1, z3), d13 = csub(z1, z3);
-      const double2 pd13 = make_double2(-d13.y, d13.x);  // i (z1 - z3)
-      a[b0] = cadd(s02, s13);
-      a[b0 + q] = cadd(d02, pd13);
-      a[b0 + 2 * q] = csub(s02, s13);
-      a[b0 + 3 * q] = csub(d02, pd13);
-    }
-    __syncthreads();
-  }
+__device__ void run_bluestein(const FftDesc &d, double2 *raw, bool inv, const TW &Wn,
+                              const TW &Wp, int P, const double2 *__restrict__ bhat) {
+  const Buf a{raw};
+  const Buf bh{const_cast<double2 *>(bhat + d.bhat)};   // read only
+  const int M = d.M, N = d.N, lg = 31 - __clz(M);
+  auto pre = [&](int j) {   // x_j c_j (conjugated input for the inverse transform)
+    double2 x = a[j];
+    if (inv) x.y = -x.y;
+    return cmul(x, chirp_of(j, d.n, N, Wn));
+  };
+  const double2 zero = make_double2(0.0, 0.0);
+  int len;
   if (lg & 1) {
     const int half = M >> 1, st = P / M;
     for (int t = threadIdx.x; t < half; t += blockDim.x) {
-      const double2 u = a[t], v = cmul(a[t + half], cconj(Wp(t * st)));
-      a[t] = cadd(u, v);
-      a[t + half] = csub(u, v);
+      const double2 u = t < N ? pre(t) : zero;
+      a[t] = u;
+      a[t + half] = cmul(u, Wp(t * st));
     }
-    __syncthreads();
-  }
-}
-
-// Input x in buf[0, N); buf holds M entries.  Result in buf[0, N).
-template <class TW>
-__device__ void run_bluestein(const FftDesc &d, double2 *raw, bool inv, const TW &Wn,
-                              const TW &wpow2, int P, const double2 *__restrict__ bhat) {
-  const double2 *bh = bhat + d.bhat;   // stored with the same swizzle as buf
-  const Buf buf{raw};
-  for (int j = threadIdx.x; j < d.M; j += blockDim.x) {
-    if (j < d.N) {
-      double2 x = buf[j];
-      if (inv) x.y = -x.y;
-      buf[j] = cmul(x, chirp_of(j, d.n, d.N, Wn));
-    } else {
-      buf[j] = make_double2(0.0, 0.0);
+    len = half;
+  } else {
+    const int q = M >> 2, st = P / M;
+    for (int t = threadIdx.x; t < q; t += blockDim.x) {
+      const double2 x0 = t < N ? pre(t) : zero;
+      const double2 x1 = t + q < N ? pre(t + q) : zero;
+      const double2 md1 = make_double2(x1.y, -x1.x);   // -i x1
+      a[t] = cadd(x0, x1);
+      a[t + q] = cmul(cadd(x0, md1), Wp(t * st));
+      a[t + 2 * q] = cmul(csub(x0, x1), Wp(2 * t * st));
+      a[t + 3 * q] = cmul(csub(x0, md1), Wp(3 * t * st));
     }
+    len = q;
   }
   __syncthreads();
-  dif_inplace(raw, d.M, wpow2, P);
-  for (int k = threadIdx.x; k < d.M; k += blockDim.x) raw[k] = cmul(raw[k], __ldg(bh + k));
+  for (; len >= 16; len >>= 2) dif_stage4(a, M, len, Wp, P);
+  for (int t = threadIdx.x; t < (M >> 2); t += blockDim.x) {
+    const int b0 = 4 * t;
+    double2 y[4];
+    {
+      const double2 x0 = a[b0], x1 = a[b0 + 1], x2 = a[b0 + 2], x3 = a[b0 + 3];
+      const double2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
+      const double2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
+      const double2 md13 = make_double2(d13.y, -d13.x);
+      y[0] = cadd(s02, s13);
+      y[1] = cadd(d02, md13);
+      y[2] = csub(s02, s13);
+      y[3] = csub(d02, md13);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) y[r] = cmul(y[r], __ldg(&bh[b0 + r]));
+    const double2 s02 = cadd(y[0], y[2]), d02 = csub(y[0], y[2]);
+    const double2 s13 = cadd(y[1], y[3]), d13 = csub(y[1], y[3]);
+    const double2 pd13 = make_double2(-d13.y, d13.x);
+    a[b0] = cadd(s02, s13);
+    a[b0 + 1] = cadd(d02, pd13);
+    a[b0 + 2] = csub(s02, s13);
+    a[b0 + 3] = csub(d02, pd13);
+  }
   __syncthreads();
-  dit_inplace_inv(raw, d.M, wpow2, P);
-  for (int k = threadIdx.x; k < d.N; k += blockDim.x) {
-    double2 y = cmul(buf[k], chirp_of(k, d.n, d.N, Wn));
+  const int top = (lg & 1) ? (M >> 1) : M;   // length of the last radix-4 stage
+  for (len = 16; len < top; len <<= 2) dit_stage4(a, M, len, Wp, P);
+  auto post = [&](int k, double2 v) {
+    double2 y = cmul(v, chirp_of(k, d.n, N, Wn));
     if (inv) y.y = -y.y;
-    buf[k] = y;
+    a[k] = y;
+  };
+  if (lg & 1) {
+    // radix-4 stages end at M/2; the radix-2 stage's outputs k < N
+    if (top >= 16) dit_stage4(a, M, top, Wp, P);
+    const int half = M >> 1, st = P / M;
+    for (int t = threadIdx.x; t < N; t += blockDim.x)
+      post(t, cadd(a[t], cmul(a[t + half], cconj(Wp(t * st)))));
+  } else {
+    // the last radix-4 stage (length M): outputs i and i + M/4 (< N <= M/2)
+    const int q = M >> 2, st = P / M;
+    for (int i = threadIdx.x; i < q; i += blockDim.x) {
+      const double2 z0 = a[i];
+      const double2 z1 = cmul(a[i + q], cconj(Wp(i * st)));
+      const double2 z2 = cmul(a[i + 2 * q], cconj(Wp(2 * i * st)));
+      const double2 z3 = cmul(a[i + 3 * q], cconj(Wp(3 * i * st)));
+      const double2 s02 = cadd(z0, z2), d02 = csub(z0, z2);
+      const double2 s13 = cadd(z1, z3), d13 = csub(z1, z3);
+      const double2 pd13 = make_double2(-d13.y, d13.x);
+      if (i < N) post(i, cadd(s02, s13));
+      if (i + q < N) post(i + q, cadd(d02, pd13));
+    }
   }
   __syncthreads();
 }
