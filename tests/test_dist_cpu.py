@@ -61,3 +61,29 @@ def test_single_process_helpers():
     import bench
     assert bench.max_over_ranks(None, torch, 0.25, "cpu") == 0.25
     assert bench.whole_job_rate(1, 12, 0.75) == pytest.approx(16.0)
+
+
+def test_clock_summary_covers_the_marked_window_only():
+    # the sampler runs for the whole benchmark; only the samples between
+    # mark() and end() describe the timed region, and a throttle reason that
+    # is active there is reported
+    sys.path.insert(0, ROOT)
+    import bench
+    clk = bench.ClockSampler(0)
+    idle = "0, 345, 1965, 120.5, 0x0, Not Active, Not Active, Not Active, Not Active"
+    busy = "0, 1965, 1965, 980.0, 0x0, Not Active, Not Active, Not Active, Not Active"
+    capped = "0, 1800, 1965, 1000.0, 0x4, Not Active, Not Active, Not Active, Active"
+    hot = "0, 1200, 1965, 700.0, 0x40, Not Active, Not Active, Active, Not Active"
+    clk.lines = [idle, idle, hot]
+    clk.mark()
+    clk.lines += [busy, capped, busy]
+    clk.end()
+    clk.lines += [idle, hot]
+    s = clk.summary()
+    assert s["samples"] == 3
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
+    clk.mark()
+    clk.lines += ["garbage", "0, [N/A], 1965, 1.0, 0x0, Not Active, Not Active, Not Active, Not Active"]
+    clk.end()
+    assert clk.summary()["samples"] == 0
