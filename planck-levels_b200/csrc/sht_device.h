@@ -195,11 +195,13 @@ void check_cuda(cudaError_t e, const char *what, const char *file, int line);
 #define SHT_CUDA(call) ::sht::check_cuda((call), #call, __FILE__, __LINE__)
 
 // Stream-ordered workspace allocation from the library's own memory pool on
-// the current device (free with cudaFreeAsync).  The pool keeps freed memory
-// mapped across synchronizes (release threshold unlimited): with the
-// device's default pool every synchronize returned the workspace to the
-// driver and the next transform mapped several GB again before its first
-// kernel.  ws_trim() hands the unused memory back (sharp_b200_release_cache).
+// the current device (free with cudaFreeAsync, never cudaFree, which leaves
+// the pool's accounting wrong).  The pool keeps freed memory mapped across
+// synchronizes (release threshold unlimited), so a transform after a
+// synchronize does not map gigabytes of workspace again, and being the
+// library's own it leaves the settings of the process's default pool alone.
+// Plan-lifetime tables use cudaMalloc.  ws_trim() hands the unused memory
+// back (sharp_b200_release_cache); ws_bytes() reports the pool's size.
 cudaError_t ws_alloc_bytes(void **p, size_t bytes, cudaStream_t st);
 template <typename T>
 inline cudaError_t ws_alloc(T **p, size_t bytes, cudaStream_t st) {
