@@ -429,3 +429,39 @@ def test_healpix_nside4096_matches_reference(ref):
     o1, o2 = run_pair(ref, ("healpix", nside), lmax, lmax, 0, 1, seed=4)
     for x, y in zip(o1, o2):
         assert rel_l2(x, y) < TOL
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_prime_ring_lengths_match_reference(ref, spin):
+    # ring lengths with large prime factors: Bluestein with convolution
+    # lengths 128 (odd number of radix-2 stages) and 256 (even), odd ring
+    # lengths, a generic radix-37 pass; paired rings of different lengths,
+    # phi0 shifts and weights; both directions against the reference
+    nph = np.array([61, 127, 122, 254, 111, 64, 97, 194], np.int32)
+    nr = len(nph)
+    theta = np.linspace(0.2, np.pi - 0.2, nr)
+    ofs = np.concatenate([[0], np.cumsum(nph)[:-1]])
+    st = np.ones(nr, np.int32)
+    phi0 = np.linspace(0.0, 0.7, nr)
+    w = np.linspace(0.5, 1.5, nr) * 4 * np.pi / nph.sum()
+    g1 = sb.Geometry.general(nph, ofs, st, phi0, theta, w)
+    g2 = ref.general(nph, ofs, st, phi0, theta, w)
+    lmax = 40
+    a1, a2 = sb.AlmInfo.triangular(lmax), ref.triangular(lmax, lmax)
+    npix = int(nph.sum())
+    na = _nalm(1, spin)
+    alms = [uniform_alm(lmax, seed=40 + i, spin=spin) for i in range(na)]
+    m1 = [np.zeros(npix) for _ in range(na)]
+    m2 = [np.zeros(npix) for _ in range(na)]
+    sb.execute(1, spin, [x.copy() for x in alms], m1, g1, a1, 1, DP)
+    ref.execute(1, spin, [x.copy() for x in alms], m2, g2, a2, 1, DP)
+    for x, y in zip(m1, m2):
+        assert rel_l2(x, y) < TOL
+    rng = np.random.default_rng(17)
+    maps = [rng.standard_normal(npix) for _ in range(na)]
+    b1 = [np.zeros_like(alms[0]) for _ in range(na)]
+    b2 = [np.zeros_like(alms[0]) for _ in range(na)]
+    sb.execute(0, spin, b1, [x.copy() for x in maps], g1, a1, 1, DP)
+    ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, DP)
+    for x, y in zip(b1, b2):
+        assert rel_l2(x, y) < TOL

@@ -124,3 +124,44 @@ def test_testsuite_lcg_alm():
     a = so.testsuite_random_alm(10, 10, 0, 1)
     assert np.all(np.abs(a.real) <= 1) and np.all(a[:11].imag == 0)
     assert len(np.unique(a.real)) > 50
+
+
+def test_oracle_prime_ring_lengths_against_reference_library():
+    # rings whose lengths have large prime factors (61, 127, 97 and twice
+    # them, 3 x 37) take the reference's Bluestein and generic-prime FFT
+    # paths, and rings shorter than 2 lmax + 1 fold aliased phases; the
+    # oracle must agree with the reference library in both directions for
+    # spins 0 and 2 on identical rings, angles and weights
+    ref = pytest.importorskip("ref")
+    if not ref.available():
+        pytest.skip("reference library not built (make -C oracle)")
+    nph = np.array([61, 127, 122, 254, 111, 64, 97, 194])
+    nr = len(nph)
+    theta = np.linspace(0.2, math.pi - 0.2, nr)
+    ofs = np.concatenate([[0], np.cumsum(nph)[:-1]])
+    stride = np.ones(nr, np.int32)
+    phi0 = np.linspace(0.0, 0.7, nr)
+    wgt = np.linspace(0.5, 1.5, nr) * 4 * math.pi / nph.sum()
+    g = ref.general(nph, ofs, stride, phi0, theta, wgt)
+    geo = so.make_geom_info(nph, ofs, stride, phi0, theta, wgt)
+    lmax = 40
+    a = ref.triangular(lmax, lmax)
+    ai = so.triangular_alm_info(lmax, lmax)
+    npix = int(nph.sum())
+    rng = np.random.default_rng(17)
+    for spin in (0, 2):
+        na = 1 if spin == 0 else 2
+        alms = [uniform_alm(lmax, seed=40 + i, spin=spin) for i in range(na)]
+        m_ref = [np.zeros(npix) for _ in range(na)]
+        m_or = [np.zeros(npix) for _ in range(na)]
+        ref.execute(1, spin, [x.copy() for x in alms], m_ref, g, a, 1, 16)
+        so.execute(1, spin, [x.copy() for x in alms], m_or, geo, ai, 1, 16)
+        for i in range(na):
+            assert rel_l2(m_or[i], m_ref[i]) < 1e-12
+        maps = [rng.standard_normal(npix) for _ in range(na)]
+        b_ref = [np.zeros_like(alms[0]) for _ in range(na)]
+        b_or = [np.zeros_like(alms[0]) for _ in range(na)]
+        ref.execute(0, spin, b_ref, [m.copy() for m in maps], g, a, 1, 16)
+        so.execute(0, spin, b_or, [m.copy() for m in maps], geo, ai, 1, 16)
+        for i in range(na):
+            assert rel_l2(b_or[i], b_ref[i]) < 1e-12
