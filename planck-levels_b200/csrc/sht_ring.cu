@@ -16,7 +16,10 @@
 // per-length table exp(-2 pi i j/n) computed once per geometry; each ring
 // copies two short slices of it into shared memory (e mod 64 and 64 (e/64))
 // and forms exp(-2 pi i e/n) as their product, so no butterfly waits on a
-// global load.
+// global load.  Lengths with large prime factors use a power-of-two
+// Bluestein convolution in place (run_bluestein).  The buffers are indexed
+// through Buf, which swizzles entries inside blocks of 8 so that the
+// butterflies' power-of-two strided accesses do not share bank groups.
 #include <cuda_runtime.h>
 
 #include <algorithm>
