@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nside", type=int, default=2048)
     ap.add_argument("--lmax", type=int, default=4096)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
                     help="headline form: batched SHARP_MIXED or the FP64 drop-in")
     ap.add_argument("--batch", type=int, default=12, help="T+QU sets per step (mixed form)")
@@ -445,7 +445,9 @@ def run_ours(args, world, rank, local, clk, np, torch, sb):
             dist.destroy_process_group()
         return
     value = whole_job_rate(world, B, step_s)
-    head_out = [x.clone() for x in sets.m[0] + sets.o[0]]
+    # outputs of every set of the headline batch (compared with FP64 below)
+    head_all = [[x.clone() for x in sets.m[i] + sets.o[i]] for i in range(B)]
+    head_out = head_all[0]
 
     # the FP64 drop-in on set 0 (ntrans = 1): companion number and the error
     # reference for the mixed outputs
@@ -453,9 +455,23 @@ def run_ours(args, world, rank, local, clk, np, torch, sb):
     fp64_s, fp64_launches, fp64_fam, _ = timed(
         torch, lib, stream, lambda: sets.step(sb, geom, ainfo, 1, DP, fp64_ops),
         args.fp64_steps if mixed else args.steps, 2, dist)
-    ref_out = sets.m[0] + sets.o[0]
-    err = {"maps": max(rel(torch, head_out[i], ref_out[i]) for i in range(3)),
-           "alms": max(rel(torch, head_out[i], ref_out[i]) for i in range(3, 6))}
+    # error of every set of the batch: the batch's round-trip outputs
+    # (mixed) against one untimed FP64 pass over all sets on the same inputs
+    err = {"maps": 0.0, "alms": 0.0, "sets": B}
+    if mixed:
+        sets.step(sb, geom, ainfo, B, DP)
+        torch.cuda.synchronize()
+        per_set = []
+        for i in range(B):
+            ref_i = sets.m[i] + sets.o[i]
+            em = max(rel(torch, head_all[i][j], ref_i[j]) for j in range(3))
+            ea = max(rel(torch, head_all[i][j], ref_i[j]) for j in range(3, 6))
+            per_set.append([em, ea])
+        err = {"maps": max(x[0] for x in per_set), "alms": max(x[1] for x in per_set),
+               "sets": B, "per_set_maps_alms": per_set,
+               "what": "max relative L2 error over the T,Q,U maps and the T,E,B round-trip "
+                       "a_lm of each set, mixed batch against FP64 on the same input a_lm"}
+    del head_all         # set 0's outputs stay referenced for the host-path check
 
     # end-to-end through sharp_execute with pinned host buffers, the same
     # batch and flags as the headline
@@ -487,20 +503,35 @@ def run_ours(args, world, rank, local, clk, np, torch, sb):
         sb.execute(sb.SHARP_MAP2ALM, 2, [x for i in hs for x in h_out[i][1:]],
                    [x for i in hs for x in h_map[i][1:]], geom, ainfo, B, flags)
 
-    # two untimed steps: every host-array call ends with a synchronize, and
-    # the second such step is where the workspace pool takes its steady size
-    for _ in range(2):
-        host_step()
-    if dist:
-        dist.barrier()
-    gc.collect()
-    gc.disable()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        host_step()
-    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-    gc.enable()
-    e2e_s = max_over_ranks(dist, torch, e2e_s, dev)
+    def host_time(fn, steps):
+        # two untimed steps: every host-array call ends with a synchronize,
+        # and the second such step is where the workspace pool takes its
+        # steady size
+        for _ in range(2):
+            fn()
+        if dist:
+            dist.barrier()
+        gc.collect()
+        gc.disable()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            fn()
+        dt = (time.perf_counter() - t0) / steps
+        gc.enable()
+        return max_over_ranks(dist, torch, dt, dev)
+
+    e2e_s = host_time(host_step, args.e2e_steps)
+
+    # the FP64 drop-in end to end: one T+QU set per step through
+    # sharp_execute with host arrays, as alm2map_pol / map2alm_pol call it
+    def host_step_fp64():
+        sb.execute(sb.SHARP_ALM2MAP, 0, [h_alm[0][0]], [h_map[0][0]], geom, ainfo, 1, DP)
+        sb.execute(sb.SHARP_ALM2MAP, 2, h_alm[0][1:], h_map[0][1:], geom, ainfo, 1, DP)
+        sb.execute(sb.SHARP_MAP2ALM, 0, [h_out[0][0]], [h_map[0][0]], geom, ainfo, 1, DP)
+        sb.execute(sb.SHARP_MAP2ALM, 2, h_out[0][1:], h_map[0][1:], geom, ainfo, 1, DP)
+
+    fp64_e2e_s = host_time(host_step_fp64, args.e2e_steps)
+    host_step()          # leave the batch's outputs in the host buffers
     h2d = B * (3 * nalm * 16 + 3 * npix * 8)
     d2h = B * (3 * npix * 8 + 3 * nalm * 16)
     t_in = sets.host[0][0]
@@ -531,8 +562,15 @@ def run_ours(args, world, rank, local, clk, np, torch, sb):
             "fp64_dropin": {"value": world / fp64_s, "unit": UNIT, "ms_per_step": fp64_s * 1e3,
                             "kernel_ms_per_step": {k: round(v[0] / (args.fp64_steps if mixed
                                                                       else args.steps), 3)
-                                                   for k, v in fp64_fam.items()}},
-            "e2e": {"value": whole_job_rate(world, B, e2e_s), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                                                   for k, v in fp64_fam.items()},
+                            "e2e": {"value": world / fp64_e2e_s, "unit": UNIT,
+                                    "steps": args.e2e_steps,
+                                    "h2d_bytes_per_step": h2d // B,
+                                    "d2h_bytes_per_step": d2h // B,
+                                    "what": "one T+QU set per step through sharp_execute with "
+                                            "host arrays (four calls, ntrans = 1)"}},
+            "e2e": {"value": whole_job_rate(world, B, e2e_s), "unit": UNIT, "steps": args.e2e_steps,
+                    "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "host_buffers": "distinct" if nh == B else "shared"},
             "gpu_launches": int(launches),
             "roofline": roof,
@@ -563,22 +601,38 @@ def roofline(dom, dom_ms, dom_n, ops, B, steps, peak):
     job = {"legendre_synth": ("s0_synth", "s2_synth"), "legendre_anal": ("s0_anal", "s2_anal"),
            "mixed_synth_spin0": ("s0_synth",), "mixed_synth_spin": ("s2_synth",),
            "mixed_anal_spin0": ("s0_anal",), "mixed_anal_spin": ("s2_anal",)}[dom]
+    leg = None
     if dom.startswith("mixed"):
         spin2 = dom.endswith("spin")
         values = ops[job[0]] / ((12 + 16 * B) if spin2 else (4 + 4 * B))
         flops_step = values * (12 if spin2 else 5) * dom_n / steps
         what = "mixed-kernel producer FP64 work (recurrence + quantisation), all launches of a step"
+        # the algorithmic count of the survey (reference opcnt of the whole
+        # B-transform job, F_leg = triples (12 + 16 B) at spin s, (4 + 4 B) at 0)
+        leg = ops[job[0]] / (dom_ms * 1e-3 / steps) / 1e12
     else:
         flops_step = sum(ops[j] for j in job)
         what = "reference operation count"
     achieved = flops_step * steps / (dom_ms * 1e-3) / 1e12
-    return {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": achieved / peak, "work": what,
-            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-            "flops_per_launch": flops_step * steps / max(dom_n, 1),
-            "ms_per_launch": dom_ms / max(dom_n, 1),
-            "launches_per_step": dom_n / steps,
-            "traffic": dram_traffic_from_profiles(dom)}
+    traffic = dram_traffic_from_profiles(dom)
+    out = {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
+           "unit": "TFLOP/s", "frac": achieved / peak, "work": what,
+           "peak_source": "cuBLAS DGEMM 8192^3 measured in this run "
+                          "(MEASURED_PEAKS.json holds no FP64 figure)",
+           "flops_per_launch": flops_step * steps / max(dom_n, 1),
+           "ms_per_launch": dom_ms / max(dom_n, 1),
+           "launches_per_step": dom_n / steps,
+           "traffic": traffic,
+           "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at "
+                              "Nside 512 / lmax 1024, scaled x16 to Nside 2048 / lmax 4096 "
+                              "(phase bytes grow with rings x (mmax+1), coefficient and a_lm "
+                              "bytes with lmax^2)") if traffic else None}
+    if leg is not None:
+        out["fp64_equivalent"] = {"achieved": leg, "frac": leg / peak,
+                                  "work": "F_leg of the job (reference opcnt, 12 + 16 ntrans "
+                                          "per (l, m, pair) at spin s, 4 + 4 ntrans at spin 0) "
+                                          "over the family's time"}
+    return out
 
 
 if __name__ == "__main__":

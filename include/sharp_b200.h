@@ -28,7 +28,12 @@ enum {
      64-bit integers and scaled to FP64 per l-tile).  Results are within
      1e-6 relative L2 of the FP64 path (typically 1e-8).  Other job types
      ignore the flag. */
-  SHARP_MIXED   = 1<<9
+  SHARP_MIXED   = 1<<9,
+  /* Subtract the result from the output arrays (maps or a_lm) instead of
+     overwriting them: the counterpart of SHARP_ADD, with which it may not be
+     combined.  It lets an iteration such as map2alm_iter form its residual
+     inside the transform instead of in a separate pass over the data. */
+  SHARP_SUBTRACT = 1<<10
 };
 
 /* Message of the last failed call on this thread ("" when none). */
@@ -48,6 +53,16 @@ void sharp_b200_execute_device (sharp_jobtype type, int spin, void *alm,
   void *map, const sharp_geom_info *geom_info, const sharp_alm_info *alm_info,
   int ntrans, int flags, void *stream, double *time,
   unsigned long long *opcnt);
+
+/* Waits for the work enqueued on `stream` (a cudaStream_t; NULL = legacy
+   default stream) and reports whether a SHARP_MIXED transform on the device
+   gave up on one of its bounded internal waits (its outputs are then not
+   valid), or whether the stream failed.  Device-pointer callers use it to
+   learn of such a failure for the call that had it; without it the failure
+   is reported at the start of the next SHARP_MIXED call.  Returns 0, or -1
+   after a failure (message in sharp_b200_last_error(); in the default abort
+   mode the failure ends the process as other errors do). */
+int sharp_b200_check_device_errors (void *stream);
 
 /* Drops the device tables cached for this geometry (sharp_destroy_geom_info
    calls it). */

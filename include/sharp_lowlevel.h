@@ -121,6 +121,24 @@ void sharp_execute (sharp_jobtype type, int spin, void *alm, void *map,
 void sharp_set_chunksize_min(int new_chunksize_min);
 void sharp_set_nchunks_max(int new_nchunks_max);
 
+/* Largest m with non-negligible Y_lm on a ring of the given sin/cos(theta)
+   (same rule as the reference).  Replaces sharp_get_mlim,
+   sharp_internal.h:64. */
+int sharp_get_mlim (int lmax, int spin, double sth, double cth);
+
+/* Vector-length hint of the low flag bits: accepted and ignored, so the
+   largest hint is 1 and the oracle answers 1.  Replace sharp_get_nv_max and
+   sharp_nv_oracle, sharp_internal.h:62-63. */
+int sharp_get_nv_max (void);
+int sharp_nv_oracle (sharp_jobtype type, int spin, int ntrans);
+
+/* Start-up banner of the reference's tools (printed to stdout), and the
+   argument-count check that prints the usage and exits(1) on a mismatch.
+   Replace sharp_announce and sharp_module_startup, sharp_announce.h:35-37. */
+void sharp_announce (const char *name);
+void sharp_module_startup (const char *name, int argc, int argc_expected,
+  const char *argv_expected, int verbose);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,9 +6,9 @@
 //   * staged a_lm  A[(moff[m] + l - m) * ncA + comp]   (double2), scaled by the
 //     recurrence normalisation c_l (and norm_l for spin > 0); each m segment
 //     is followed by kPad zero entries so l-blocks may run past lmax;
-//   * phase       P[((m * npairs + p) * ncm + comp) * 2 + hemisphere] (double2);
-//     the two hemispheres of one (m, pair, comp) are adjacent (one 32-byte
-//     sector) so the ring FFT reads them together.
+//   * phase       P[((p * ncm + comp) * 2 + hemisphere) * (mmax + 1) + m]
+//     (double2): ring-major, so the ring FFT reads and writes contiguous rows
+//     and the Legendre kernels write one element per (m, pair, comp, ring).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,6 +34,29 @@ struct FftDesc {
   int M;
   long long bhat;  // offset of the transformed chirp (digit order of the DIF stages, /M)
 };
+
+// Host half of a geometry plan (build_geom_host, no device calls): what the
+// cached plans upload and the allocation-free synthesis places in its fixed
+// scratch.  Pairs are in internal (decreasing mlim) order; per-ring entries
+// are indexed 2*p + hemisphere.
+struct GeomHost {
+  int npairs = 0, nphmax = 0, nmax_complex = 0;
+  int P = 2;                          // largest Bluestein convolution length (>= 2)
+  int synth_tile = 256;
+  std::vector<int> order, count_m, mlim_sorted;
+  std::vector<int2> synth_items, mixed_items;
+  std::vector<double> cth, sth, phi0, weight;
+  std::vector<int> nph, stride, fft;
+  std::vector<long long> ofs;
+  std::vector<FftDesc> descs;
+  std::vector<int> tw_n, tw_off;      // per distinct length: n and table offset
+  std::vector<int> blue_idx;          // descriptors that use Bluestein
+  long long tw_total = 0, bhat_total = 0;
+  std::vector<int> cls_N, cls_start, cls_count, cls_bufA, cls_bufB, cls_pairs;
+  long long map_lo = 0, map_hi = 0;
+  bool map_covered = false;
+};
+GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin);
 
 // Per-geometry device tables (pairs in internal mlim order).
 struct GeomPlan {

@@ -32,6 +32,9 @@ void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
 
 namespace {
 
+// flags whose jobs update the output arrays instead of overwriting them
+constexpr int kAccumulate = SHARP_ADD | SHARP_SUBTRACT;
+
 // ---------------------------------------------------------------------------
 // small helpers
 // ---------------------------------------------------------------------------
@@ -150,75 +153,73 @@ bool ws_bytes(unsigned long long *reserved, unsigned long long *used) {
   return true;
 }
 
-namespace {
-
 // ---------------------------------------------------------------------------
-// geometry plan
+// Host half of a geometry plan (no device calls): pairs in decreasing mlim
+// order, the per-m counts and work lists, per-ring tables, one FFT
+// descriptor per distinct ring length (radices, Bluestein choice, twiddle and
+// chirp offsets) and the FFT size classes.  The cached plans and the
+// allocation-free synthesis both build on it.
 // ---------------------------------------------------------------------------
-std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, int mmax, int spin,
-                                          cudaStream_t st) {
-  auto gp = std::make_unique<GeomPlan>();
-  gp->key = g;
-  gp->hash = hash_geom(g);
-  gp->lmax = lmax;
-  gp->mmax = mmax;
-  gp->spin = spin;
+GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin) {
+  GeomHost h;
   const int np = g->npairs;
-  gp->npairs = np;
-  gp->nphmax = g->nphmax;
+  h.npairs = np;
+  h.nphmax = g->nphmax;
   std::vector<int> mlim(np);
   for (int i = 0; i < np; ++i) mlim[i] = get_mlim(lmax, spin, g->pair[i].r1.sth, g->pair[i].r1.cth);
-  gp->order.resize(np);
-  std::iota(gp->order.begin(), gp->order.end(), 0);
-  std::stable_sort(gp->order.begin(), gp->order.end(),
+  h.order.resize(np);
+  std::iota(h.order.begin(), h.order.end(), 0);
+  std::stable_sort(h.order.begin(), h.order.end(),
                    [&](int a, int b) { return mlim[a] > mlim[b]; });
   // count_m[m] = number of pairs with mlim >= m (a prefix of the sorted order)
   std::vector<int> hist(mmax + 1, 0);
   for (int i = 0; i < np; ++i)
     if (mlim[i] >= 0) hist[std::min(mlim[i], mmax)] += 1;
-  gp->count_m.assign(mmax + 1, 0);
+  h.count_m.assign(mmax + 1, 0);
   int run = 0;
   for (int m = mmax; m >= 0; --m) {
     run += hist[m];
-    gp->count_m[m] = run;
+    h.count_m[m] = run;
   }
-  gp->synth_tile = 256;
   for (int m = 0; m <= mmax; ++m)
-    for (int t = 0; t * gp->synth_tile < gp->count_m[m]; ++t) gp->synth_items.push_back({m, t});
+    for (int t = 0; t * h.synth_tile < h.count_m[m]; ++t) h.synth_items.push_back({m, t});
   for (int m = 0; m <= mmax; ++m)
-    for (int t = 0; t * 256 < gp->count_m[m]; ++t) gp->mixed_items.push_back({m, t});
+    for (int t = 0; t * 256 < h.count_m[m]; ++t) h.mixed_items.push_back({m, t});
 
-  std::vector<double> cth(np), sth(np), phi0(2 * np), weight(2 * np);
-  std::vector<int> ml_sorted(np), nph(2 * np), stride(2 * np), fft(2 * np, 0);
-  std::vector<long long> ofs(2 * np);
+  h.cth.resize(np);
+  h.sth.resize(np);
+  h.mlim_sorted.resize(np);
+  h.phi0.resize(2 * np);
+  h.weight.resize(2 * np);
+  h.nph.resize(2 * np);
+  h.stride.resize(2 * np);
+  h.fft.assign(2 * np, 0);
+  h.ofs.resize(2 * np);
   std::map<int, int> len_index;
-  std::vector<FftDesc> descs;
-  long long tw_total = 0;
-  std::vector<int> tw_n, tw_off;
   long long lo = 0, hi = 0;
   bool first = true, unit_stride = true;
   std::vector<std::pair<long long, long long>> spans;
   for (int p = 0; p < np; ++p) {
-    const sharp_ringpair &pr = g->pair[gp->order[p]];
-    cth[p] = pr.r1.cth;
-    sth[p] = pr.r1.sth;
-    ml_sorted[p] = mlim[gp->order[p]];
-    for (int h = 0; h < 2; ++h) {
-      const sharp_ringinfo &r = h ? pr.r2 : pr.r1;
-      const int i = 2 * p + h;
-      const bool present = (h == 0) || r.nph > 0;
-      nph[i] = present ? r.nph : -1;
-      phi0[i] = present ? r.phi0 : 0.0;
-      weight[i] = present ? r.weight : 0.0;
-      ofs[i] = present ? r.ofs : 0;
-      stride[i] = present ? r.stride : 1;
+    const sharp_ringpair &pr = g->pair[h.order[p]];
+    h.cth[p] = pr.r1.cth;
+    h.sth[p] = pr.r1.sth;
+    h.mlim_sorted[p] = mlim[h.order[p]];
+    for (int hh = 0; hh < 2; ++hh) {
+      const sharp_ringinfo &r = hh ? pr.r2 : pr.r1;
+      const int i = 2 * p + hh;
+      const bool present = (hh == 0) || r.nph > 0;
+      h.nph[i] = present ? r.nph : -1;
+      h.phi0[i] = present ? r.phi0 : 0.0;
+      h.weight[i] = present ? r.weight : 0.0;
+      h.ofs[i] = present ? r.ofs : 0;
+      h.stride[i] = present ? r.stride : 1;
       if (!present || r.nph <= 0) continue;
       auto it = len_index.find(r.nph);
       if (it == len_index.end()) {
         FftDesc d{};
         d.n = r.nph;
         d.N = (r.nph & 1) ? r.nph : r.nph / 2;
-        d.tw = int(tw_total);
+        d.tw = int(h.tw_total);
         auto rad = factor_fft(d.N);
         SHT_REQUIRE(int(rad.size()) <= kMaxRadices, "ring length has too many factors");
         d.nrad = int(rad.size());
@@ -226,7 +227,7 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
         // Stockham cost ~ N * sum(generic radices); Bluestein ~ M log2 M + 2N
         // (power-of-two convolution of length M >= 2N-1)
         long long direct = 0;
-        for (int r : rad) direct += (r > 5 && r != 8) ? r : 1;
+        for (int rr : rad) direct += (rr > 5 && rr != 8) ? rr : 1;
         direct *= d.N;
         int M = 1, lg = 0;
         while (M < 2 * d.N - 1) { M <<= 1; ++lg; }
@@ -234,14 +235,14 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
         d.blue = (d.N > 16 && blue_cost < direct) ? 1 : 0;
         d.M = d.blue ? M : 0;
         d.bhat = 0;
-        tw_n.push_back(d.n);
-        tw_off.push_back(int(tw_total));
-        tw_total += d.n;
-        it = len_index.emplace(r.nph, int(descs.size())).first;
-        descs.push_back(d);
-        gp->nmax_complex = std::max(gp->nmax_complex, d.N);
+        h.tw_n.push_back(d.n);
+        h.tw_off.push_back(int(h.tw_total));
+        h.tw_total += d.n;
+        it = len_index.emplace(r.nph, int(h.descs.size())).first;
+        h.descs.push_back(d);
+        h.nmax_complex = std::max(h.nmax_complex, d.N);
       }
-      fft[i] = it->second;
+      h.fft[i] = it->second;
       const long long a = r.ofs, b = r.ofs + (long long)(r.nph - 1) * r.stride;
       const long long rlo = std::min(a, b), rhi = std::max(a, b) + 1;
       if (first) { lo = rlo; hi = rhi; first = false; }
@@ -251,84 +252,115 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
       spans.push_back({rlo, rhi});
     }
   }
-  SHT_REQUIRE(tw_total < (1ll << 31), "geometry too large (twiddle table)");
-  long long bhat_total = 0;
-  for (auto &d : descs)
-    if (d.blue) {
-      d.bhat = bhat_total;
-      bhat_total += d.M;
-      gp->P = std::max(gp->P, d.M);
-    }
+  SHT_REQUIRE(h.tw_total < (1ll << 31), "geometry too large (twiddle table)");
+  for (int i = 0; i < int(h.descs.size()); ++i) {
+    FftDesc &d = h.descs[i];
+    if (!d.blue) continue;
+    d.bhat = h.bhat_total;
+    h.bhat_total += d.M;
+    h.P = std::max(h.P, d.M);
+    h.blue_idx.push_back(i);
+  }
   // rings tile [lo,hi) exactly -> synthesis need not pre-load the map
   bool covered = unit_stride && !spans.empty();
   if (covered) {
     std::sort(spans.begin(), spans.end());
     long long cur = lo;
-    for (auto &s : spans) {
-      if (s.first != cur) { covered = false; break; }
-      cur = s.second;
+    for (auto &sp : spans) {
+      if (sp.first != cur) { covered = false; break; }
+      cur = sp.second;
     }
     covered = covered && cur == hi;
   }
-  gp->map_lo = lo;
-  gp->map_hi = hi;
-  gp->map_covered = covered;
+  h.map_lo = lo;
+  h.map_hi = hi;
+  h.map_covered = covered;
   // FFT size classes (the last class is capped by shared memory)
-  {
-    const int bounds[4] = {256, 1024, 4096, gp->nmax_complex};
-    std::vector<std::vector<int>> lists(4);
-    for (int p = 0; p < np; ++p) {
-      int nmx = 0;
-      for (int h = 0; h < 2; ++h)
-        if (nph[2 * p + h] > 0) nmx = std::max(nmx, descs[fft[2 * p + h]].N);
-      int c = 0;
-      while (c < 3 && nmx > bounds[c]) ++c;
-      lists[c].push_back(p);
-    }
-    std::vector<int> flat;
-    for (int c = 0; c < 4; ++c) {
-      // shared memory: buffer A holds N+2 (Stockham) or M (Bluestein)
-      // entries, buffer B N+2
-      int bufA = 2, bufB = 2;
-      for (int p : lists[c])
-        for (int h = 0; h < 2; ++h)
-          if (nph[2 * p + h] > 0) {
-            const FftDesc &d = descs[fft[2 * p + h]];
-            bufA = std::max(bufA, d.blue ? std::max(d.M, d.N + 2) : d.N + 2);
-            bufB = std::max(bufB, d.N + 2);
-          }
-      // whole blocks of 8 entries: the ring kernels swizzle indices inside them
-      bufA = (bufA + 7) & ~7;
-      bufB = (bufB + 7) & ~7;
-      gp->cls_N.push_back(std::max(bounds[c], 1));
-      gp->cls_bufA.push_back(bufA);
-      gp->cls_bufB.push_back(bufB);
-      gp->cls_start.push_back(int(flat.size()));
-      gp->cls_count.push_back(int(lists[c].size()));
-      flat.insert(flat.end(), lists[c].begin(), lists[c].end());
-      // classes whose buffers exceed shared memory run them in global scratch
-    }
-    gp->cls_pairs = dev_upload(flat, st);
+  const int bounds[4] = {256, 1024, 4096, h.nmax_complex};
+  std::vector<std::vector<int>> lists(4);
+  for (int p = 0; p < np; ++p) {
+    int nmx = 0;
+    for (int hh = 0; hh < 2; ++hh)
+      if (h.nph[2 * p + hh] > 0) nmx = std::max(nmx, h.descs[h.fft[2 * p + hh]].N);
+    int c = 0;
+    while (c < 3 && nmx > bounds[c]) ++c;
+    lists[c].push_back(p);
   }
+  for (int c = 0; c < 4; ++c) {
+    // shared memory: buffer A holds N+2 (Stockham) or M (Bluestein)
+    // entries, buffer B N+2
+    int bufA = 2, bufB = 2;
+    for (int p : lists[c])
+      for (int hh = 0; hh < 2; ++hh)
+        if (h.nph[2 * p + hh] > 0) {
+          const FftDesc &d = h.descs[h.fft[2 * p + hh]];
+          bufA = std::max(bufA, d.blue ? std::max(d.M, d.N + 2) : d.N + 2);
+          bufB = std::max(bufB, d.N + 2);
+        }
+    // whole blocks of 8 entries: the ring kernels swizzle indices inside them
+    bufA = (bufA + 7) & ~7;
+    bufB = (bufB + 7) & ~7;
+    h.cls_N.push_back(std::max(bounds[c], 1));
+    h.cls_bufA.push_back(bufA);
+    h.cls_bufB.push_back(bufB);
+    h.cls_start.push_back(int(h.cls_pairs.size()));
+    h.cls_count.push_back(int(lists[c].size()));
+    h.cls_pairs.insert(h.cls_pairs.end(), lists[c].begin(), lists[c].end());
+    // classes whose buffers exceed shared memory run them in global scratch
+  }
+  return h;
+}
 
-  gp->cth = dev_upload(cth, st);
-  gp->sth = dev_upload(sth, st);
-  gp->mlim = dev_upload(ml_sorted, st);
+namespace {
+
+// ---------------------------------------------------------------------------
+// geometry plan
+// ---------------------------------------------------------------------------
+std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, int mmax, int spin,
+                                          cudaStream_t st) {
+  const GeomHost h = build_geom_host(g, lmax, mmax, spin);
+  auto gp = std::make_unique<GeomPlan>();
+  gp->key = g;
+  gp->hash = hash_geom(g);
+  gp->lmax = lmax;
+  gp->mmax = mmax;
+  gp->spin = spin;
+  gp->npairs = h.npairs;
+  gp->nphmax = h.nphmax;
+  gp->nmax_complex = h.nmax_complex;
+  gp->count_m = h.count_m;
+  gp->order = h.order;
+  gp->synth_items = h.synth_items;
+  gp->synth_tile = h.synth_tile;
+  gp->mixed_items = h.mixed_items;
+  gp->P = h.P;
+  gp->cls_N = h.cls_N;
+  gp->cls_start = h.cls_start;
+  gp->cls_count = h.cls_count;
+  gp->cls_bufA = h.cls_bufA;
+  gp->cls_bufB = h.cls_bufB;
+  gp->map_lo = h.map_lo;
+  gp->map_hi = h.map_hi;
+  gp->map_covered = h.map_covered;
+  gp->cls_pairs = dev_upload(h.cls_pairs, st);
+  gp->cth = dev_upload(h.cth, st);
+  gp->sth = dev_upload(h.sth, st);
+  gp->mlim = dev_upload(h.mlim_sorted, st);
   gp->count = dev_upload(gp->count_m, st);
   gp->items = dev_upload(gp->synth_items, st);
   gp->mitems = dev_upload(gp->mixed_items, st);
-  gp->phi0 = dev_upload(phi0, st);
-  gp->weight = dev_upload(weight, st);
-  gp->ofs = dev_upload(ofs, st);
-  gp->nph = dev_upload(nph, st);
-  gp->stride = dev_upload(stride, st);
-  gp->fft = dev_upload(fft, st);
-  gp->fdesc = dev_upload(descs, st);
-  SHT_CUDA(cudaMalloc(&gp->twiddle, sizeof(double2) * std::max<long long>(tw_total, 1)));
-  launch_twiddles(*gp, int(tw_total), tw_n, tw_off, st);
-  SHT_CUDA(cudaMalloc(&gp->bhat, sizeof(double2) * std::max<long long>(bhat_total, 1)));
+  gp->phi0 = dev_upload(h.phi0, st);
+  gp->weight = dev_upload(h.weight, st);
+  gp->ofs = dev_upload(h.ofs, st);
+  gp->nph = dev_upload(h.nph, st);
+  gp->stride = dev_upload(h.stride, st);
+  gp->fft = dev_upload(h.fft, st);
+  gp->fdesc = dev_upload(h.descs, st);
+  SHT_CUDA(cudaMalloc(&gp->twiddle, sizeof(double2) * std::max<long long>(h.tw_total, 1)));
+  launch_twiddles(*gp, int(h.tw_total), h.tw_n, h.tw_off, st);
+  SHT_CUDA(cudaMalloc(&gp->bhat, sizeof(double2) * std::max<long long>(h.bhat_total, 1)));
   SHT_CUDA(cudaMalloc(&gp->wpow2, sizeof(double2) * gp->P));
-  launch_bluestein_setup(*gp, descs, st);
+  launch_bluestein_setup(*gp, h.descs, st);
   SHT_CUDA(cudaStreamSynchronize(st));
   return gp;
 }
@@ -560,6 +592,8 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
     flags |= SHARP_USE_WEIGHTS;
   }
   SHT_REQUIRE(spin >= 0 && spin <= ainfo->lmax, "bad spin");
+  SHT_REQUIRE((flags & kAccumulate) != kAccumulate,
+              "SHARP_ADD and SHARP_SUBTRACT exclude each other");
   SHT_REQUIRE(!(flags & SHARP_MIXED) || (type == SHARP_ALM2MAP && spin == 0) ||
                   type == SHARP_MAP2ALM || type == SHARP_ALM2MAP,
               "SHARP_MIXED applies to alm2map and map2alm jobs");
@@ -638,8 +672,8 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
   } else {
     map_lo = gp->map_lo;
     alm_lo = ap->lo;
-    const bool load_maps = analysis || (flags & SHARP_ADD) || !gp->map_covered;
-    const bool load_alm = !analysis || (flags & SHARP_ADD) || !ap->covered;
+    const bool load_maps = analysis || (flags & kAccumulate) || !gp->map_covered;
+    const bool load_alm = !analysis || (flags & kAccumulate) || !ap->covered;
     for (int i = 0; i < nmapptr; ++i) {
       owned.emplace_back(new DevBuf(esz_map * map_n, st));
       dmap[i] = owned.back()->p;
@@ -809,8 +843,8 @@ bool execute_pipelined(sharp_jobtype type, int spin, void *alm, void *map,
   }
   const size_t esz_map = dp ? 8 : 4, esz_alm = (dp ? 8 : 4) * (packed ? 1 : 2);
   const long long map_n = map_hi - map_lo, alm_n = alm_hi - alm_lo;
-  const bool load_maps = analysis || (flags & SHARP_ADD) || !map_covered;
-  const bool load_alm = !analysis || (flags & SHARP_ADD) || !alm_covered;
+  const bool load_maps = analysis || (flags & kAccumulate) || !map_covered;
+  const bool load_alm = !analysis || (flags & kAccumulate) || !alm_covered;
   void **alm_in = static_cast<void **>(alm);
   void **map_in = static_cast<void **>(map);
   cudaStream_t sin = copy_stream(0), sout = copy_stream(1);
@@ -1033,6 +1067,16 @@ void sharp_b200_release_cache(void) {
   // workspace freed in stream order is unused once the device is idle
   cudaDeviceSynchronize();
   sht::ws_trim();
+}
+
+int sharp_b200_check_device_errors(void *stream) {
+  int rc = -1;
+  sht::guarded([&] {
+    SHT_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    sht::check_tc_error();
+    rc = 0;
+  });
+  return rc;
 }
 
 int sharp_b200_workspace_bytes(unsigned long long *reserved, unsigned long long *used) {

@@ -418,4 +418,43 @@ static int g_chunksize_min = 500, g_nchunks_max = 10;
 void sharp_set_chunksize_min(int v) { g_chunksize_min = v; }
 void sharp_set_nchunks_max(int v) { g_nchunks_max = v; }
 
+// ---------------------------------------------------------------------------
+// Helpers the reference exports beside the job interface (its test suite and
+// tools call them): the m cut-off of a ring, the vector-length hint and its
+// autotuner, and the start-up banner.
+// ---------------------------------------------------------------------------
+int sharp_get_mlim(int lmax, int spin, double sth, double cth) {
+  return sht::get_mlim(lmax, spin, sth, cth);
+}
+
+// The low flag bits of a job select the reference's SIMD vector count (1..6);
+// this engine has one kernel variant per job shape, so every hint is the same
+// and the autotuner answers 1 without running anything.
+int sharp_get_nv_max(void) { return 1; }
+int sharp_nv_oracle(sharp_jobtype type, int spin, int ntrans) {
+  if (type == SHARP_ALM2MAP_DERIV1) spin = 1;
+  if (!(int(type) >= 0 && int(type) < 5)) fail(__FILE__, __LINE__, "bad type");
+  if (ntrans <= 0) fail(__FILE__, __LINE__, "bad number of simultaneous transforms");
+  if (spin < 0) fail(__FILE__, __LINE__, "bad spin");
+  return 1;
+}
+
+void sharp_announce(const char *name) {
+  const size_t n = std::strlen(name);
+  std::printf("\n+-");
+  for (size_t i = 0; i < n; ++i) std::printf("-");
+  std::printf("-+\n| %s |\n+-", name);
+  for (size_t i = 0; i < n; ++i) std::printf("-");
+  std::printf("-+\n\n");
+  std::printf("Spherical-harmonic transforms: libsharp_b200 (CUDA, sm_100a)\n\n");
+}
+
+void sharp_module_startup(const char *name, int argc, int argc_expected,
+                          const char *argv_expected, int verbose) {
+  if (verbose) sharp_announce(name);
+  if (argc == argc_expected) return;
+  if (verbose) std::fprintf(stderr, "Usage: %s %s\n", name, argv_expected);
+  std::exit(1);
+}
+
 }  // extern "C"

@@ -69,16 +69,6 @@ struct Layout {
   }
 };
 
-std::vector<int> factors(int N) {
-  std::vector<int> r;
-  int n = N;
-  while (n % 4 == 0) { r.push_back(4); n /= 4; }
-  while (n % 2 == 0) { r.push_back(2); n /= 2; }
-  for (int p = 3; n > 1; p += 2)
-    while (n % p == 0) { r.push_back(p); n /= p; }
-  return r;
-}
-
 int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const void *alm,
                     void *map, cudaStream_t st) {
   SHT_REQUIRE(g != nullptr && a != nullptr && alm != nullptr && map != nullptr,
@@ -96,113 +86,19 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   }
   SHT_REQUIRE(mmax <= lmax, "incorrect l_max: must be >= m_max");
 
-  // ---- host tables: pairs in decreasing mlim order -------------------------
-  const int np = g->npairs;
-  std::vector<int> mlim(np), order(np);
-  for (int i = 0; i < np; ++i) mlim[i] = get_mlim(lmax, 0, g->pair[i].r1.sth, g->pair[i].r1.cth);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return mlim[x] > mlim[y]; });
-  std::vector<int> count(mmax + 1, 0), hist(mmax + 1, 0);
-  for (int i = 0; i < np; ++i)
-    if (mlim[i] >= 0) hist[std::min(mlim[i], mmax)] += 1;
-  for (int m = mmax, run = 0; m >= 0; --m) count[m] = (run += hist[m]);
-  const int tile = 256;
-  std::vector<int2> items;
-  for (int m = 0; m <= mmax; ++m)
-    for (int t = 0; t * tile < count[m]; ++t) items.push_back({m, t});
-
-  std::vector<double> cth(np), sth(np), phi0(2 * np), weight(2 * np);
-  std::vector<int> mls(np), nph(2 * np), stride(2 * np), fft(2 * np, 0);
-  std::vector<long long> ofs(2 * np);
-  std::map<int, int> len_index;
-  std::vector<FftDesc> descs;
-  std::vector<int> tw_n, tw_off, blue_idx;
-  long long tw_total = 0, bhat_total = 0;
-  int P = 2;
-  for (int p = 0; p < np; ++p) {
-    const sharp_ringpair &pr = g->pair[order[p]];
-    cth[p] = pr.r1.cth;
-    sth[p] = pr.r1.sth;
-    mls[p] = mlim[order[p]];
-    for (int h = 0; h < 2; ++h) {
-      const sharp_ringinfo &r = h ? pr.r2 : pr.r1;
-      const int i = 2 * p + h;
-      const bool present = (h == 0) || r.nph > 0;
-      nph[i] = present ? r.nph : -1;
-      phi0[i] = present ? r.phi0 : 0.0;
-      weight[i] = present ? r.weight : 0.0;
-      ofs[i] = present ? r.ofs : 0;
-      stride[i] = present ? r.stride : 1;
-      if (!present || r.nph <= 0) continue;
-      auto it = len_index.find(r.nph);
-      if (it == len_index.end()) {
-        FftDesc d{};
-        d.n = r.nph;
-        d.N = (r.nph & 1) ? r.nph : r.nph / 2;
-        d.tw = int(tw_total);
-        const auto rad = factors(d.N);
-        SHT_REQUIRE(int(rad.size()) <= kMaxRadices, "ring length has too many factors");
-        d.nrad = int(rad.size());
-        for (int k = 0; k < d.nrad; ++k) d.rad[k] = rad[k];
-        long long direct = 0;
-        for (int rr : rad) direct += (rr > 5) ? rr : 1;
-        direct *= d.N;
-        int M = 1, lg = 0;
-        while (M < 2 * d.N - 1) { M <<= 1; ++lg; }
-        d.blue = (d.N > 16 && 2ll * ((long long)M * lg + 2ll * d.N) < direct) ? 1 : 0;
-        d.M = d.blue ? M : 0;
-        d.bhat = 0;
-        if (d.blue) {
-          d.bhat = bhat_total;
-          bhat_total += M;
-          P = std::max(P, M);
-          blue_idx.push_back(int(descs.size()));
-        }
-        tw_n.push_back(d.n);
-        tw_off.push_back(int(tw_total));
-        tw_total += d.n;
-        it = len_index.emplace(r.nph, int(descs.size())).first;
-        descs.push_back(d);
-      }
-      fft[i] = it->second;
+  // ---- host tables (the same builder as the cached plans) --------------------
+  const GeomHost h = build_geom_host(g, lmax, mmax, 0);
+  const int np = h.npairs;
+  // every size class must run its FFT buffers in shared memory: the
+  // global-scratch variant of the ring kernels allocates workspace
+  for (int c = 0; c < int(h.cls_N.size()); ++c)
+    if (h.cls_count[c] > 0 &&
+        sizeof(double2) * ring_fft_smem_entries(h.cls_bufA[c], h.cls_bufB[c], mmax,
+                                                h.nmax_complex, h.P) > 227 * 1024) {
+      record_error("sharp_b200_alm2map_noalloc: ring lengths above the shared-memory FFT "
+                   "limit need workspace; use sharp_b200_execute_device instead");
+      return -1;
     }
-  }
-  // FFT size classes
-  const int bounds[4] = {256, 1024, 4096, 1 << 30};
-  std::vector<std::vector<int>> lists(4);
-  for (int p = 0; p < np; ++p) {
-    int nmx = 0;
-    for (int h = 0; h < 2; ++h)
-      if (nph[2 * p + h] > 0) nmx = std::max(nmx, descs[fft[2 * p + h]].N);
-    int c = 0;
-    while (c < 3 && nmx > bounds[c]) ++c;
-    lists[c].push_back(p);
-  }
-  std::vector<int> flat, cls_N, cls_start, cls_count, cls_bufA, cls_bufB;
-  int nmax_all = 1;
-  for (const FftDesc &d : descs) nmax_all = std::max(nmax_all, d.N);
-  for (int c = 0; c < 4; ++c) {
-    int bufA = 2, bufB = 2, nmaxc = 1;
-    for (int p : lists[c])
-      for (int h = 0; h < 2; ++h)
-        if (nph[2 * p + h] > 0) {
-          const FftDesc &d = descs[fft[2 * p + h]];
-          bufA = std::max(bufA, d.blue ? std::max(d.M, d.N + 2) : d.N + 2);
-          bufB = std::max(bufB, d.N + 2);
-          nmaxc = std::max(nmaxc, d.N);
-        }
-    cls_N.push_back(std::min(bounds[c], std::max(nmaxc, 1)));
-    bufA = (bufA + 7) & ~7;   // whole blocks of 8 (swizzled in the ring kernels)
-    bufB = (bufB + 7) & ~7;
-    cls_bufA.push_back(bufA);
-    cls_bufB.push_back(bufB);
-    cls_start.push_back(int(flat.size()));
-    cls_count.push_back(int(lists[c].size()));
-    flat.insert(flat.end(), lists[c].begin(), lists[c].end());
-    SHT_REQUIRE(sizeof(double2) * ring_fft_smem_entries(bufA, bufB, mmax, nmax_all, P) <=
-                    227 * 1024,
-                "ring length exceeds the shared-memory FFT limit");
-  }
   // recurrence tables
   std::vector<long long> moff(mmax + 2);
   long long off = 0;
@@ -222,18 +118,18 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   Layout L;
   const size_t o_cth = L.take<double>(np), o_sth = L.take<double>(np);
   const size_t o_mlim = L.take<int>(np), o_count = L.take<int>(mmax + 1);
-  const size_t o_items = L.take<int2>(items.size());
+  const size_t o_items = L.take<int2>(h.synth_items.size());
   const size_t o_phi0 = L.take<double>(2 * np), o_weight = L.take<double>(2 * np);
   const size_t o_ofs = L.take<long long>(2 * np);
   const size_t o_nph = L.take<int>(2 * np), o_stride = L.take<int>(2 * np);
   const size_t o_fft = L.take<int>(2 * np);
-  const size_t o_fdesc = L.take<FftDesc>(descs.size());
-  const size_t o_cls = L.take<int>(flat.size());
-  const size_t o_twn = L.take<int>(tw_n.size()), o_twoff = L.take<int>(tw_off.size());
-  const size_t o_blue = L.take<int>(blue_idx.size());
-  const size_t o_tw = L.take<double2>(tw_total);
-  const size_t o_wp = L.take<double2>(P);
-  const size_t o_bhat = L.take<double2>(bhat_total);
+  const size_t o_fdesc = L.take<FftDesc>(h.descs.size());
+  const size_t o_cls = L.take<int>(h.cls_pairs.size());
+  const size_t o_twn = L.take<int>(h.tw_n.size()), o_twoff = L.take<int>(h.tw_off.size());
+  const size_t o_blue = L.take<int>(h.blue_idx.size());
+  const size_t o_tw = L.take<double2>(h.tw_total);
+  const size_t o_wp = L.take<double2>(h.P);
+  const size_t o_bhat = L.take<double2>(h.bhat_total);
   const size_t o_moff = L.take<long long>(mmax + 2);
   const size_t o_alpha = L.take<double>(off), o_cfac = L.take<double>(off);
   const size_t o_mfac = L.take<double>(mmax + 1);
@@ -255,22 +151,22 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   auto put = [&](size_t o, const void *src, size_t bytes) {
     if (bytes) SHT_CUDA(cudaMemcpyAsync(at(o), src, bytes, cudaMemcpyHostToDevice, st));
   };
-  put(o_cth, cth.data(), sizeof(double) * np);
-  put(o_sth, sth.data(), sizeof(double) * np);
-  put(o_mlim, mls.data(), sizeof(int) * np);
-  put(o_count, count.data(), sizeof(int) * (mmax + 1));
-  put(o_items, items.data(), sizeof(int2) * items.size());
-  put(o_phi0, phi0.data(), sizeof(double) * 2 * np);
-  put(o_weight, weight.data(), sizeof(double) * 2 * np);
-  put(o_ofs, ofs.data(), sizeof(long long) * 2 * np);
-  put(o_nph, nph.data(), sizeof(int) * 2 * np);
-  put(o_stride, stride.data(), sizeof(int) * 2 * np);
-  put(o_fft, fft.data(), sizeof(int) * 2 * np);
-  put(o_fdesc, descs.data(), sizeof(FftDesc) * descs.size());
-  put(o_cls, flat.data(), sizeof(int) * flat.size());
-  put(o_twn, tw_n.data(), sizeof(int) * tw_n.size());
-  put(o_twoff, tw_off.data(), sizeof(int) * tw_off.size());
-  put(o_blue, blue_idx.data(), sizeof(int) * blue_idx.size());
+  put(o_cth, h.cth.data(), sizeof(double) * np);
+  put(o_sth, h.sth.data(), sizeof(double) * np);
+  put(o_mlim, h.mlim_sorted.data(), sizeof(int) * np);
+  put(o_count, h.count_m.data(), sizeof(int) * (mmax + 1));
+  put(o_items, h.synth_items.data(), sizeof(int2) * h.synth_items.size());
+  put(o_phi0, h.phi0.data(), sizeof(double) * 2 * np);
+  put(o_weight, h.weight.data(), sizeof(double) * 2 * np);
+  put(o_ofs, h.ofs.data(), sizeof(long long) * 2 * np);
+  put(o_nph, h.nph.data(), sizeof(int) * 2 * np);
+  put(o_stride, h.stride.data(), sizeof(int) * 2 * np);
+  put(o_fft, h.fft.data(), sizeof(int) * 2 * np);
+  put(o_fdesc, h.descs.data(), sizeof(FftDesc) * h.descs.size());
+  put(o_cls, h.cls_pairs.data(), sizeof(int) * h.cls_pairs.size());
+  put(o_twn, h.tw_n.data(), sizeof(int) * h.tw_n.size());
+  put(o_twoff, h.tw_off.data(), sizeof(int) * h.tw_off.size());
+  put(o_blue, h.blue_idx.data(), sizeof(int) * h.blue_idx.size());
   put(o_moff, moff.data(), sizeof(long long) * (mmax + 2));
   put(o_mfac, mfac.data(), sizeof(double) * (mmax + 1));
   put(o_mvs, mvstart.data(), sizeof(long long) * (mmax + 1));
@@ -294,9 +190,9 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
       a.mvstart = nullptr;
     }
   } release{gp, cp, ap};
-  gp.lmax = lmax; gp.mmax = mmax; gp.spin = 0; gp.npairs = np; gp.nphmax = g->nphmax;
-  gp.nmax_complex = nmax_all;
-  gp.count_m = count; gp.synth_items = items; gp.synth_tile = tile;
+  gp.lmax = lmax; gp.mmax = mmax; gp.spin = 0; gp.npairs = np; gp.nphmax = h.nphmax;
+  gp.nmax_complex = h.nmax_complex;
+  gp.count_m = h.count_m; gp.synth_items = h.synth_items; gp.synth_tile = h.synth_tile;
   gp.cth = static_cast<double *>(at(o_cth)); gp.sth = static_cast<double *>(at(o_sth));
   gp.mlim = static_cast<int *>(at(o_mlim)); gp.count = static_cast<int *>(at(o_count));
   gp.items = static_cast<int2 *>(at(o_items));
@@ -305,9 +201,9 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   gp.nph = static_cast<int *>(at(o_nph)); gp.stride = static_cast<int *>(at(o_stride));
   gp.fft = static_cast<int *>(at(o_fft)); gp.fdesc = static_cast<FftDesc *>(at(o_fdesc));
   gp.twiddle = static_cast<double2 *>(at(o_tw)); gp.wpow2 = static_cast<double2 *>(at(o_wp));
-  gp.bhat = static_cast<double2 *>(at(o_bhat)); gp.P = P;
-  gp.cls_N = cls_N; gp.cls_start = cls_start; gp.cls_count = cls_count;
-  gp.cls_bufA = cls_bufA; gp.cls_bufB = cls_bufB;
+  gp.bhat = static_cast<double2 *>(at(o_bhat)); gp.P = h.P;
+  gp.cls_N = h.cls_N; gp.cls_start = h.cls_start; gp.cls_count = h.cls_count;
+  gp.cls_bufA = h.cls_bufA; gp.cls_bufB = h.cls_bufB;
   gp.cls_pairs = static_cast<int *>(at(o_cls));
   cp.lmax = lmax; cp.mmax = mmax; cp.spin = 0; cp.total = off; cp.moff = moff;
   cp.d_moff = static_cast<long long *>(at(o_moff));
@@ -322,13 +218,14 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
 
   // ---- the transform ---------------------------------------------------------
   launch_twiddles_preplaced(gp.twiddle, static_cast<int *>(at(o_twn)),
-                            static_cast<int *>(at(o_twoff)), int(tw_n.size()), st);
+                            static_cast<int *>(at(o_twoff)), int(h.tw_n.size()), st);
   // power-of-two table exp(-2 pi i j/P) of the Bluestein passes
-  const int pw[2] = {P, 0};  // length, offset
+  const int pw[2] = {h.P, 0};  // length, offset
   put(o_pw, pw, sizeof(pw));
   launch_twiddles_preplaced(gp.wpow2, static_cast<int *>(at(o_pw)),
                             static_cast<int *>(at(o_pw)) + 1, 1, st);
-  launch_bluestein_setup_preplaced(gp, static_cast<int *>(at(o_blue)), int(blue_idx.size()), st);
+  launch_bluestein_setup_preplaced(gp, static_cast<int *>(at(o_blue)), int(h.blue_idx.size()),
+                                   st);
   launch_coef_tables(cp, st);
   auto *ptr_dev = static_cast<void *const *>(at(o_ptr));
   launch_stage_alm(job, ap, 0, cp, static_cast<double *>(at(o_norm)), ptr_dev, 1,

@@ -485,8 +485,10 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
                                   int nitems) {
   extern __shared__ double2 smem[];
   const int ms = mmax + 1;
-  const bool add = (flags & SHARP_ADD) != 0;
-  const double wscale = (flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0;
+  // SHARP_SUBTRACT: the negated result is added (negation is exact)
+  const bool add = (flags & (SHARP_ADD | SHARP_SUBTRACT)) != 0;
+  const double wscale = ((flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0) *
+                        ((flags & SHARP_SUBTRACT) ? -1.0 : 1.0);
   // buffers A/B in shared memory, or (rings too long for it) in this CTA's
   // slot of a global scratch; such CTAs loop over (pair, component) items
   const bool gb = gbuf != nullptr;
@@ -688,7 +690,7 @@ __global__ void phase2ring_direct_kernel(const int *__restrict__ mlim, const int
                                          long long map_lo) {
   const int p = blockIdx.x, c = blockIdx.y;
   const int mm = min(mmax, mlim[p]);
-  const bool add = (flags & SHARP_ADD) != 0;
+  const bool add = (flags & (SHARP_ADD | SHARP_SUBTRACT)) != 0;
   T2 *map = maps[c];
   for (int h = 0; h < 2; ++h) {
     const int ring = 2 * p + h;
@@ -696,6 +698,7 @@ __global__ void phase2ring_direct_kernel(const int *__restrict__ mlim, const int
     if (n <= 0) continue;
     double wgt = (flags & SHARP_USE_WEIGHTS) ? n * weight[ring] : 1.0;
     if (flags & SHARP_REAL_HARMONICS) wgt *= kSqrtHalf;
+    if (flags & SHARP_SUBTRACT) wgt = -wgt;
     const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * (mmax + 1);
     for (int m = threadIdx.x; m <= mmax; m += blockDim.x) {
       const double2 v = (m <= mm) ? cscale(src[m], wgt) : make_double2(0.0, 0.0);
@@ -786,8 +789,9 @@ __global__ void scatter_alm_kernel(int lmax, int nalmptr, const long long *__res
                                    const long long *__restrict__ moff,
                                    const double *__restrict__ cfac,
                                    const double *__restrict__ norm_l, bool use_norm,
-                                   double norm_m0, bool add, const double *__restrict__ Aout,
-                                   int ncA, T *const *__restrict__ alm) {
+                                   double norm_m0, double sgn, bool add,
+                                   const double *__restrict__ Aout, int ncA,
+                                   T *const *__restrict__ alm) {
   const int m = blockIdx.x;
   const long long mo = moff[m] - m;
   const long long base = mvstart[m];
@@ -796,7 +800,7 @@ __global__ void scatter_alm_kernel(int lmax, int nalmptr, const long long *__res
     const int l = m + e / nalmptr;
     const int c = e % nalmptr;
     const double *src = Aout + ((mo + l) * ncA + c) * 2;
-    double f = cfac[mo + l];
+    double f = cfac[mo + l] * sgn;
     if (use_norm) f *= norm_l[l];
     double vr = src[0] * f, vi = src[1] * f;
     T *a = alm[c];
@@ -1054,17 +1058,19 @@ void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
                         void *const *alm_dev, int nalmptr, cudaStream_t st) {
   const bool use_norm = job.spin > 0 || job.type == SHARP_ALM2MAP_DERIV1;
   const double norm_m0 = (job.flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0;
-  const bool add = (job.flags & SHARP_ADD) != 0;
+  // SHARP_SUBTRACT: the negated result is added (negation is exact)
+  const double sgn = (job.flags & SHARP_SUBTRACT) ? -1.0 : 1.0;
+  const bool add = (job.flags & (SHARP_ADD | SHARP_SUBTRACT)) != 0;
   const int blocks = job.mmax + 1;
   ProfScope ps("scatter_alm", st);
   if (job.dp)
     scatter_alm_kernel<double><<<blocks, 256, 0, st>>>(
         job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
-        use_norm, norm_m0, add, Aout, ncA, reinterpret_cast<double *const *>(alm_dev));
+        use_norm, norm_m0, sgn, add, Aout, ncA, reinterpret_cast<double *const *>(alm_dev));
   else
     scatter_alm_kernel<float><<<blocks, 256, 0, st>>>(
         job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
-        use_norm, norm_m0, add, Aout, ncA, reinterpret_cast<float *const *>(alm_dev));
+        use_norm, norm_m0, sgn, add, Aout, ncA, reinterpret_cast<float *const *>(alm_dev));
   SHT_CUDA(cudaGetLastError());
 }
 

@@ -29,6 +29,7 @@ SHARP_REAL_HARMONICS = 1 << 6
 SHARP_NO_FFT = 1 << 7
 SHARP_ADJOINT = 1 << 8
 SHARP_MIXED = 1 << 9
+SHARP_SUBTRACT = 1 << 10
 SHARP_PACKED = 1
 
 
@@ -107,6 +108,22 @@ def workspace_bytes():
     r, u = C.c_ulonglong(0), C.c_ulonglong(0)
     _lib.sharp_b200_workspace_bytes(C.byref(r), C.byref(u))
     return r.value, u.value
+
+
+_lib.sharp_b200_check_device_errors.argtypes = [C.c_void_p]
+_lib.sharp_b200_check_device_errors.restype = C.c_int
+
+
+def check_device_errors(stream=None) -> None:
+    """sharp_b200_check_device_errors: waits for ``stream`` (a
+    torch.cuda.Stream; default torch's current stream) and raises SharpError
+    if a SHARP_MIXED transform enqueued there gave up on a bounded wait or the
+    stream failed."""
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    _lib.sharp_b200_check_device_errors(C.c_void_p(stream.cuda_stream))
+    _check()
 
 
 def last_error() -> str:

@@ -12,13 +12,26 @@ flag of sharp_b200.h), not autograd of a reimplementation:
 
 Tensors: a_lm complex128 (triangular m-major layout, one tensor per
 component), maps float64, all on the same CUDA device.
+
+precision="mixed" runs the forward transform and its adjoint with
+SHARP_MIXED (the int8 tensor-core Legendre step, within 1e-6 relative L2 of
+FP64); precision="fp64" (default) runs both in FP64.
 """
 from __future__ import annotations
 
 import torch
 
-from . import (SHARP_ADJOINT, SHARP_ALM2MAP, SHARP_DP, SHARP_MAP2ALM, AlmInfo, Geometry,
-               execute_device)
+from . import (SHARP_ADJOINT, SHARP_ALM2MAP, SHARP_DP, SHARP_MAP2ALM, SHARP_MIXED, AlmInfo,
+               Geometry, execute_device)
+
+_PRECISION = {"fp64": SHARP_DP, "mixed": SHARP_DP | SHARP_MIXED}
+
+
+def _flags(precision: str) -> int:
+    try:
+        return _PRECISION[precision]
+    except KeyError:
+        raise ValueError(f"precision must be one of {sorted(_PRECISION)}") from None
 
 
 def _real(t: torch.Tensor) -> torch.Tensor:
@@ -35,13 +48,13 @@ def _m_weights(lmax: int, mmax: int, device) -> torch.Tensor:
 
 class _Alm2Map(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, geom: Geometry, ainfo: AlmInfo, spin: int, npix: int, *alms):
-        ctx.geom, ctx.ainfo, ctx.spin = geom, ainfo, spin
+    def forward(ctx, geom: Geometry, ainfo: AlmInfo, spin: int, npix: int, flags: int, *alms):
+        ctx.geom, ctx.ainfo, ctx.spin, ctx.flags = geom, ainfo, spin, flags
         maps = [torch.empty(npix, dtype=torch.float64, device=alms[0].device)
                 for _ in alms]
         alm_in = [a.detach().contiguous() for a in alms]  # Im a_l0 is ignored by Y
         execute_device(SHARP_ALM2MAP, spin, [_real(a) for a in alm_in], maps, geom, ainfo, 1,
-                       SHARP_DP)
+                       flags)
         return tuple(maps) if len(maps) > 1 else maps[0]
 
     @staticmethod
@@ -53,20 +66,20 @@ class _Alm2Map(torch.autograd.Function):
                 for _ in gm]
         # Yt through the adjoint flag on the synthesis job type
         execute_device(SHARP_ALM2MAP, spin, [_real(a) for a in galm], gm, geom, ainfo, 1,
-                       SHARP_DP | SHARP_ADJOINT)
+                       ctx.flags | SHARP_ADJOINT)
         w = _m_weights(lmax, nm - 1, gm[0].device)
         galm = [a * w for a in galm]
-        return (None, None, None, None, *galm)
+        return (None, None, None, None, None, *galm)
 
 
 class _Map2Alm(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, geom: Geometry, ainfo: AlmInfo, spin: int, *maps):
-        ctx.geom, ctx.ainfo, ctx.spin = geom, ainfo, spin
+    def forward(ctx, geom: Geometry, ainfo: AlmInfo, spin: int, flags: int, *maps):
+        ctx.geom, ctx.ainfo, ctx.spin, ctx.flags = geom, ainfo, spin, flags
         alms = [torch.zeros(ainfo.nalm(), dtype=torch.complex128, device=maps[0].device)
                 for _ in maps]
         execute_device(SHARP_MAP2ALM, spin, [_real(a) for a in alms],
-                       [m.detach().contiguous() for m in maps], geom, ainfo, 1, SHARP_DP)
+                       [m.detach().contiguous() for m in maps], geom, ainfo, 1, flags)
         return tuple(alms) if len(alms) > 1 else alms[0]
 
     @staticmethod
@@ -79,16 +92,18 @@ class _Map2Alm(torch.autograd.Function):
         gmaps = [torch.zeros(npix, dtype=torch.float64, device=ga[0].device) for _ in ga]
         # (Yt W)^T = W Y: the adjoint of the analysis job type
         execute_device(SHARP_MAP2ALM, spin, [_real(a) for a in ga], gmaps, geom, ainfo, 1,
-                       SHARP_DP | SHARP_ADJOINT)
-        return (None, None, None, *gmaps)
+                       ctx.flags | SHARP_ADJOINT)
+        return (None, None, None, None, *gmaps)
 
 
-def alm2map(geom: Geometry, ainfo: AlmInfo, spin: int, *alms: torch.Tensor):
+def alm2map(geom: Geometry, ainfo: AlmInfo, spin: int, *alms: torch.Tensor,
+            precision: str = "fp64"):
     """Differentiable synthesis: spin 0 takes one a_lm tensor, spin > 0 two
     (E, B); returns one map or a (Q, U) tuple."""
-    return _Alm2Map.apply(geom, ainfo, spin, geom.npix(), *alms)
+    return _Alm2Map.apply(geom, ainfo, spin, geom.npix(), _flags(precision), *alms)
 
 
-def map2alm(geom: Geometry, ainfo: AlmInfo, spin: int, *maps: torch.Tensor):
+def map2alm(geom: Geometry, ainfo: AlmInfo, spin: int, *maps: torch.Tensor,
+            precision: str = "fp64"):
     """Differentiable analysis (with the geometry's quadrature weights)."""
-    return _Map2Alm.apply(geom, ainfo, spin, *maps)
+    return _Map2Alm.apply(geom, ainfo, spin, _flags(precision), *maps)

@@ -1,9 +1,12 @@
 """sharp_b200_execute_batch: a batch of independent jobs of uneven HEALPix
-resolution, lmax and spin (the shape of the batched configuration: spin-0
-and spin-2 TEB -> IQU sets with Nside drawn from a small set and
-lmax = 2 Nside, E/B spectra 0.1 and 0.01 of T), at sizes the tests finish in
-seconds.  Each output must equal sharp_execute on its own job (FP64), and the
+resolution, lmax and spin (the batched configuration: spin-0 and spin-2
+TEB -> IQU sets with Nside drawn from a small set and lmax = 2 Nside, E/B
+spectra 0.1 and 0.01 of T), at small sizes and at the configuration's own
+size (48 spin-0 + 16 spin-2 sets, Nside 256/512/1024).  Each output must
+equal sharp_execute on its own job (FP64) and the reference, and the
 SHARP_MIXED batch must stay within 1e-6 relative L2 of FP64 per map."""
+import time
+
 import numpy as np
 import pytest
 
@@ -155,3 +158,43 @@ def test_batch_device_pointers_and_merge_limit():
         sb.execute(sb.SHARP_ALM2MAP, 0, [alms[i].copy()], ref_map, g, a, 1, DP)
         assert rel_l2(tm[i].cpu().numpy(), ref_map[0]) < 1e-13
 
+
+def test_config2_full_size_per_map_errors():
+    # the batched configuration at its stated size: 48 spin-0 + 16 spin-2
+    # sets, Nside uniform over {256, 512, 1024}, lmax = 2 Nside, one batch
+    # call per direction and precision.  FP64 against the reference on a
+    # subset of sets (1e-12); SHARP_MIXED against FP64 on every map (1e-6),
+    # the per-map errors printed.
+    import ref
+    geo, sets = _mix(nsides=(256, 512, 1024), n0=48, n2=16, seed=5)
+    alms = [s[2] for s in sets]
+    t0 = time.perf_counter()
+    _, m64 = _run_batch(geo, sets, sb.SHARP_ALM2MAP, DP, alms)
+    t1 = time.perf_counter()
+    _, mmx = _run_batch(geo, sets, sb.SHARP_ALM2MAP, DP | MIXED, alms)
+    t2 = time.perf_counter()
+    _, a64 = _run_batch(geo, sets, sb.SHARP_MAP2ALM, DP, m64)
+    _, amx = _run_batch(geo, sets, sb.SHARP_MAP2ALM, DP | MIXED, m64)
+    emap = [rel_l2(x, y) for xb, yb in zip(mmx, m64) for x, y in zip(xb, yb)]
+    ealm = [rel_l2(x, y) for xb, yb in zip(amx, a64) for x, y in zip(xb, yb)]
+    print(f"config 2: {len(sets)} sets, {len(emap)} maps; host-array batch alm2map "
+          f"FP64 {t1 - t0:.2f} s, mixed {t2 - t1:.2f} s; mixed vs FP64 per map: "
+          f"maps max {max(emap):.2e} median {np.median(emap):.2e}, "
+          f"a_lm max {max(ealm):.2e} median {np.median(ealm):.2e}")
+    assert max(emap) < TOL_MIXED and max(ealm) < TOL_MIXED
+    if not ref.available():
+        pytest.skip("reference library not built (make -C oracle)")
+    # reference on one spin-0 and one spin-2 set of each resolution
+    pick = {}
+    for i, (spin, n, _) in enumerate(sets):
+        pick.setdefault((spin, n), i)
+    for (spin, n), i in sorted(pick.items()):
+        g, a = ref.healpix(n), ref.triangular(2 * n, 2 * n)
+        out = [np.zeros(12 * n * n) for _ in alms[i]]
+        ref.execute(sb.SHARP_ALM2MAP, spin, [x.copy() for x in alms[i]], out, g, a, 1, DP)
+        for x, y in zip(m64[i], out):
+            assert rel_l2(x, y) < 1e-12
+        back = [np.zeros_like(x) for x in alms[i]]
+        ref.execute(sb.SHARP_MAP2ALM, spin, back, [x.copy() for x in m64[i]], g, a, 1, DP)
+        for x, y in zip(a64[i], back):
+            assert rel_l2(x, y) < 1e-12

@@ -358,6 +358,47 @@ def test_metric_config_nside2048_lmax4096_spin0_and_spin2(ref):
     sb.execute(0, 2, x1, [q2.copy(), u2.copy()], g1, a1, 1, DP)
     ref.execute(0, 2, x2, [q2.copy(), u2.copy()], g2, a2, 1, DP)
     assert rel_l2(x1[0], x2[0]) < TOL and rel_l2(x1[1], x2[1]) < TOL
+    # spin-0 analysis of the reference's T map
+    y1, y2 = np.zeros_like(t), np.zeros_like(t)
+    sb.execute(0, 0, [y1], [m2.copy()], g1, a1, 1, DP)
+    ref.execute(0, 0, [y2], [m2.copy()], g2, a2, 1, DP)
+    assert rel_l2(y1, y2) < TOL
+
+
+def test_config4_nside4096_lmax8192_fp64_matches_reference(ref):
+    # the large polarised configuration in FP64 against the reference:
+    # Nside 4096 (rings up to 16384 pixels), lmax = mmax = 8192, spin 0 and 2,
+    # both directions, with its spectra (C_l^T with a 1-arcmin beam, E and B
+    # at 0.1 and 0.01 of it).  This pins the scaled run-up of the recurrence
+    # for m up to 8192 on the reference itself (libsharp/sharp_core_inc.c).
+    nside, lmax = 4096, 8192
+    g1, g2 = sb.Geometry.healpix(nside), ref.healpix(nside)
+    a1, a2 = sb.AlmInfo.triangular(lmax), ref.triangular(lmax, lmax)
+    cl = cl_spectrum(lmax, beam_arcmin=1.0)
+    rng = np.random.default_rng(41)
+    npix = 12 * nside * nside
+    t = random_alm(lmax, cl=cl, rng=rng)
+    m1, m2 = np.zeros(npix), np.zeros(npix)
+    sb.execute(1, 0, [t.copy()], [m1], g1, a1, 1, DP)
+    ref.execute(1, 0, [t.copy()], [m2], g2, a2, 1, DP)
+    assert rel_l2(m1, m2) < TOL
+    y1, y2 = np.zeros_like(t), np.zeros_like(t)
+    sb.execute(0, 0, [y1], [m2], g1, a1, 1, DP)
+    ref.execute(0, 0, [y2], [m2], g2, a2, 1, DP)
+    assert rel_l2(y1, y2) < TOL
+    del t, m1, m2, y1, y2
+    e = random_alm(lmax, cl=0.1 * cl, rng=rng)
+    b = random_alm(lmax, cl=0.01 * cl, rng=rng)
+    q1, u1, q2, u2 = (np.zeros(npix) for _ in range(4))
+    sb.execute(1, 2, [e.copy(), b.copy()], [q1, u1], g1, a1, 1, DP)
+    ref.execute(1, 2, [e.copy(), b.copy()], [q2, u2], g2, a2, 1, DP)
+    assert rel_l2(q1, q2) < TOL and rel_l2(u1, u2) < TOL
+    del q1, u1
+    x1 = [np.zeros_like(e), np.zeros_like(e)]
+    x2 = [np.zeros_like(e), np.zeros_like(e)]
+    sb.execute(0, 2, x1, [q2, u2], g1, a1, 1, DP)
+    ref.execute(0, 2, x2, [q2, u2], g2, a2, 1, DP)
+    assert rel_l2(x1[0], x2[0]) < TOL and rel_l2(x1[1], x2[1]) < TOL
 
 
 def test_results_are_bitwise_repeatable():

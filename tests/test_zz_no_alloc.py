@@ -62,3 +62,27 @@ def test_noalloc_refuses_problems_above_its_scratch():
     assert rc == -1
     assert "MiB of scratch" in sb.last_error()
     sb.clear_error()
+
+
+def test_noalloc_allocates_no_device_memory():
+    # the point of the entry point: after a first call on the device (which
+    # looks up the array's address and loads the kernels), further calls
+    # leave the library's workspace pool and the device's free memory exactly
+    # as they were
+    import torch
+    f = _entry()
+    nside, lmax = 128, 256
+    g, a = sb.Geometry.healpix(nside), sb.AlmInfo.triangular(lmax)
+    alm = torch.from_numpy(random_alm(lmax, seed=3).view(np.float64).copy()).cuda()
+    got = torch.zeros(12 * nside * nside, dtype=torch.float64, device="cuda")
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    args = (g.ptr, a.ptr, C.c_void_p(alm.data_ptr()), C.c_void_p(got.data_ptr()), st)
+    assert f(*args) == 0, sb.last_error()
+    torch.cuda.synchronize()
+    pool0 = sb.workspace_bytes()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        assert f(*args) == 0, sb.last_error()
+    torch.cuda.synchronize()
+    assert sb.workspace_bytes() == pool0
+    assert torch.cuda.mem_get_info()[0] == free0
