@@ -807,48 +807,43 @@ cudaStream_t copy_stream(int which) {
   return s;
 }
 
-bool execute_pipelined(sharp_jobtype type, int spin, void *alm, void *map,
-                       const sharp_geom_info *ginfo, const sharp_alm_info *ainfo, int ntrans,
-                       int flags, double *time, unsigned long long *opcnt) {
+// A host-array job the pipelined path can take (checked like execute_impl
+// would; anything else goes through execute_impl, which reports the error).
+bool pipelinable(sharp_jobtype type, int spin, const void *alm, const void *map,
+                 const sharp_geom_info *ginfo, const sharp_alm_info *ainfo, int ntrans,
+                 int flags) {
   if (type != SHARP_ALM2MAP && type != SHARP_MAP2ALM) return false;
   if (flags & (SHARP_ADJOINT | SHARP_NO_FFT)) return false;
-  if (!ginfo || !ainfo || !alm || !map || ntrans < 2 || ntrans > kMaxTrans) return false;
+  if ((flags & kAccumulate) == kAccumulate) return false;
+  if (!ginfo || !ainfo || !alm || !map || ntrans < 1 || ntrans > kMaxTrans) return false;
   if (spin < 0 || spin > ainfo->lmax || ainfo->nm < 1 || ainfo->nm - 1 > ainfo->lmax) return false;
-  {
-    // every m exactly once (otherwise the plain path reports the error)
-    std::vector<char> seen(ainfo->nm, 0);
-    for (int i = 0; i < ainfo->nm; ++i) {
-      const int mv = ainfo->mval[i];
-      if (mv < 0 || mv >= ainfo->nm || seen[mv]) return false;
-      seen[mv] = 1;
-    }
+  // every m exactly once (otherwise the plain path reports the error)
+  std::vector<char> seen(ainfo->nm, 0);
+  for (int i = 0; i < ainfo->nm; ++i) {
+    const int mv = ainfo->mval[i];
+    if (mv < 0 || mv >= ainfo->nm || seen[mv]) return false;
+    seen[mv] = 1;
   }
-  const bool analysis = type == SHARP_MAP2ALM;
-  // piece size: the transforms one launch of the batched kernels takes
-  const int piece = spin > 0 ? 3 : (analysis ? 6 : 4);
-  if (ntrans <= piece) return false;
-  const double t0 = wall_now();
-  const int ncomp = spin > 0 ? 2 : 1;       // maps and a_lm per transform
-  const bool dp = (flags & SHARP_DP) != 0;
-  long long map_lo, map_hi, alm_lo, alm_hi;
-  bool map_covered, alm_covered, packed;
-  cudaStream_t cs = library_stream();
-  {
-    std::lock_guard<std::mutex> lk(g_cache_mutex);
-    const int mmax = ainfo->nm - 1;
-    GeomPlan *gp = get_geom_plan(ginfo, ainfo->lmax, mmax, spin, cs);
-    AlmPlan *ap = get_alm_plan(ainfo, mmax, cs);
-    map_lo = gp->map_lo; map_hi = gp->map_hi; map_covered = gp->map_covered;
-    alm_lo = ap->lo; alm_hi = ap->hi; alm_covered = ap->covered; packed = ap->packed;
-  }
-  const size_t esz_map = dp ? 8 : 4, esz_alm = (dp ? 8 : 4) * (packed ? 1 : 2);
-  const long long map_n = map_hi - map_lo, alm_n = alm_hi - alm_lo;
-  const bool load_maps = analysis || (flags & kAccumulate) || !map_covered;
-  const bool load_alm = !analysis || (flags & kAccumulate) || !alm_covered;
-  void **alm_in = static_cast<void **>(alm);
-  void **map_in = static_cast<void **>(map);
-  cudaStream_t sin = copy_stream(0), sout = copy_stream(1);
+  return true;
+}
 
+struct HostJob {
+  sharp_jobtype type;
+  int spin;
+  void *alm, *map;
+  const sharp_geom_info *ginfo;
+  const sharp_alm_info *ainfo;
+  int ntrans, flags;
+};
+
+// Runs host-array jobs as one sequence of pieces (see above): the copies of
+// consecutive pieces overlap the compute across job boundaries too, so a
+// list of jobs has one fill and one drain.  Every job must satisfy
+// pipelinable(); the jobs must be independent (no job reads another's
+// output).  *opcnt receives the summed operation count of the jobs.
+void execute_pipelined_jobs(const std::vector<HostJob> &jobs, unsigned long long *opcnt) {
+  cudaStream_t cs = library_stream();
+  cudaStream_t sin = copy_stream(0), sout = copy_stream(1);
   // window buffers of one piece, released on the output stream after its copies
   struct Piece {
     std::vector<void *> dmap, dalm;
@@ -864,75 +859,115 @@ bool execute_pipelined(sharp_jobtype type, int spin, void *alm, void *map,
     }
     pieces.clear();
   };
-  unsigned long long first_ops = 0;
+  unsigned long long total_ops = 0;
+  bool any_mixed = false;
   try {
-    for (int t0p = 0; t0p < ntrans; t0p += piece) {
-      const int nt = std::min(piece, ntrans - t0p);
-      pieces.emplace_back();
-      Piece &pc = pieces.back();
-      pc.dmap.assign(size_t(nt) * ncomp, nullptr);
-      pc.dalm.assign(size_t(nt) * ncomp, nullptr);
-      SHT_CUDA(cudaEventCreateWithFlags(&pc.in_done, cudaEventDisableTiming));
-      SHT_CUDA(cudaEventCreateWithFlags(&pc.compute_done, cudaEventDisableTiming));
-      // inputs of the piece: host -> device on the input stream
-      for (int i = 0; i < nt * ncomp; ++i) {
-        const int gi = t0p * ncomp + i;
-        SHT_CUDA(::sht::ws_alloc(&pc.dmap[i], esz_map * std::max<long long>(map_n, 1), sin));
-        SHT_CUDA(::sht::ws_alloc(&pc.dalm[i], esz_alm * std::max<long long>(alm_n, 1), sin));
-        if (load_maps && map_n > 0)
-          SHT_CUDA(cudaMemcpyAsync(pc.dmap[i], static_cast<char *>(map_in[gi]) + esz_map * map_lo,
-                                   esz_map * map_n, cudaMemcpyHostToDevice, sin));
-        if (load_alm && alm_n > 0)
-          SHT_CUDA(cudaMemcpyAsync(pc.dalm[i], static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
-                                   esz_alm * alm_n, cudaMemcpyHostToDevice, sin));
+    for (const HostJob &jb : jobs) {
+      const sharp_jobtype type = jb.type;
+      const int spin = jb.spin, ntrans = jb.ntrans, flags = jb.flags;
+      const sharp_geom_info *ginfo = jb.ginfo;
+      const sharp_alm_info *ainfo = jb.ainfo;
+      any_mixed = any_mixed || (flags & SHARP_MIXED);
+      const bool analysis = type == SHARP_MAP2ALM;
+      // piece size: the transforms one launch of the batched kernels takes
+      const int piece = spin > 0 ? 3 : (analysis ? 6 : 4);
+      const int ncomp = spin > 0 ? 2 : 1;       // maps and a_lm per transform
+      const bool dp = (flags & SHARP_DP) != 0;
+      long long map_lo, map_hi, alm_lo, alm_hi;
+      bool map_covered, alm_covered, packed;
+      {
+        std::lock_guard<std::mutex> lk(g_cache_mutex);
+        const int mmax = ainfo->nm - 1;
+        GeomPlan *gp = get_geom_plan(ginfo, ainfo->lmax, mmax, spin, cs);
+        AlmPlan *ap = get_alm_plan(ainfo, mmax, cs);
+        map_lo = gp->map_lo; map_hi = gp->map_hi; map_covered = gp->map_covered;
+        alm_lo = ap->lo; alm_hi = ap->hi; alm_covered = ap->covered; packed = ap->packed;
       }
-      SHT_CUDA(cudaEventRecord(pc.in_done, sin));
-      // compute on the library stream: a device-pointer job whose array
-      // bases are placed so that element lo sits at the start of each window
-      SHT_CUDA(cudaStreamWaitEvent(cs, pc.in_done, 0));
-      std::vector<void *> bm(nt * ncomp), ba(nt * ncomp);
-      for (int i = 0; i < nt * ncomp; ++i) {
-        bm[i] = static_cast<char *>(pc.dmap[i]) - esz_map * map_lo;
-        ba[i] = static_cast<char *>(pc.dalm[i]) - esz_alm * alm_lo;
-      }
-      unsigned long long oc = 0;
-      execute_impl(type, spin, ba.data(), bm.data(), ginfo, ainfo, nt, flags, true, cs, nullptr,
-                   &oc);
-      if (t0p == 0) first_ops = oc;
-      SHT_CUDA(cudaEventRecord(pc.compute_done, cs));
-      // outputs of the piece: device -> host on the output stream
-      SHT_CUDA(cudaStreamWaitEvent(sout, pc.compute_done, 0));
-      for (int i = 0; i < nt * ncomp; ++i) {
-        const int gi = t0p * ncomp + i;
-        if (analysis) {
-          if (alm_n > 0)
-            SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
-                                     pc.dalm[i], esz_alm * alm_n, cudaMemcpyDeviceToHost, sout));
-        } else if (map_n > 0) {
-          SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(map_in[gi]) + esz_map * map_lo,
-                                   pc.dmap[i], esz_map * map_n, cudaMemcpyDeviceToHost, sout));
+      const size_t esz_map = dp ? 8 : 4, esz_alm = (dp ? 8 : 4) * (packed ? 1 : 2);
+      const long long map_n = map_hi - map_lo, alm_n = alm_hi - alm_lo;
+      const bool load_maps = analysis || (flags & kAccumulate) || !map_covered;
+      const bool load_alm = !analysis || (flags & kAccumulate) || !alm_covered;
+      void **alm_in = static_cast<void **>(jb.alm);
+      void **map_in = static_cast<void **>(jb.map);
+      unsigned long long first_ops = 0;
+      for (int t0p = 0; t0p < ntrans; t0p += piece) {
+        const int nt = std::min(piece, ntrans - t0p);
+        pieces.emplace_back();
+        Piece &pc = pieces.back();
+        pc.dmap.assign(size_t(nt) * ncomp, nullptr);
+        pc.dalm.assign(size_t(nt) * ncomp, nullptr);
+        SHT_CUDA(cudaEventCreateWithFlags(&pc.in_done, cudaEventDisableTiming));
+        SHT_CUDA(cudaEventCreateWithFlags(&pc.compute_done, cudaEventDisableTiming));
+        // inputs of the piece: host -> device on the input stream
+        for (int i = 0; i < nt * ncomp; ++i) {
+          const int gi = t0p * ncomp + i;
+          SHT_CUDA(::sht::ws_alloc(&pc.dmap[i], esz_map * std::max<long long>(map_n, 1), sin));
+          SHT_CUDA(::sht::ws_alloc(&pc.dalm[i], esz_alm * std::max<long long>(alm_n, 1), sin));
+          if (load_maps && map_n > 0)
+            SHT_CUDA(cudaMemcpyAsync(pc.dmap[i], static_cast<char *>(map_in[gi]) + esz_map * map_lo,
+                                     esz_map * map_n, cudaMemcpyHostToDevice, sin));
+          if (load_alm && alm_n > 0)
+            SHT_CUDA(cudaMemcpyAsync(pc.dalm[i], static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
+                                     esz_alm * alm_n, cudaMemcpyHostToDevice, sin));
+        }
+        SHT_CUDA(cudaEventRecord(pc.in_done, sin));
+        // compute on the library stream: a device-pointer job whose array
+        // bases are placed so that element lo sits at the start of each window
+        SHT_CUDA(cudaStreamWaitEvent(cs, pc.in_done, 0));
+        std::vector<void *> bm(nt * ncomp), ba(nt * ncomp);
+        for (int i = 0; i < nt * ncomp; ++i) {
+          bm[i] = static_cast<char *>(pc.dmap[i]) - esz_map * map_lo;
+          ba[i] = static_cast<char *>(pc.dalm[i]) - esz_alm * alm_lo;
+        }
+        unsigned long long oc = 0;
+        execute_impl(type, spin, ba.data(), bm.data(), ginfo, ainfo, nt, flags, true, cs,
+                     nullptr, &oc);
+        if (t0p == 0) first_ops = oc;
+        SHT_CUDA(cudaEventRecord(pc.compute_done, cs));
+        // outputs of the piece: device -> host on the output stream
+        SHT_CUDA(cudaStreamWaitEvent(sout, pc.compute_done, 0));
+        for (int i = 0; i < nt * ncomp; ++i) {
+          const int gi = t0p * ncomp + i;
+          if (analysis) {
+            if (alm_n > 0)
+              SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
+                                       pc.dalm[i], esz_alm * alm_n, cudaMemcpyDeviceToHost, sout));
+          } else if (map_n > 0) {
+            SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(map_in[gi]) + esz_map * map_lo,
+                                     pc.dmap[i], esz_map * map_n, cudaMemcpyDeviceToHost, sout));
+          }
         }
       }
+      // the count of one call with all transforms (per-triple weight of
+      // sharp_core_inc2.c:173,442): the pieces share the triples
+      const int n0 = std::min(piece, ntrans);
+      const unsigned long long c0 = spin == 0 ? 4 + 4ull * n0 : 12 + 16ull * n0;
+      const unsigned long long c = spin == 0 ? 4 + 4ull * ntrans : 12 + 16ull * ntrans;
+      total_ops += (first_ops / c0) * c;
     }
     release();
     SHT_CUDA(cudaStreamSynchronize(sout));
     SHT_CUDA(cudaStreamSynchronize(cs));
-    if (flags & SHARP_MIXED) check_tc_error();
+    if (any_mixed) check_tc_error();
   } catch (const Failure &) {
     release();
     cudaStreamSynchronize(sout);
     cudaStreamSynchronize(cs);
     throw;
   }
-  if (opcnt) {
-    // the count of one call with all transforms (per-triple weight of
-    // sharp_core_inc2.c:173,442): the pieces share the triples
-    const int n0 = std::min(piece, ntrans);
-    const unsigned long long c0 = spin == 0 ? 4 + 4ull * n0 : 12 + 16ull * n0;
-    const unsigned long long c = spin == 0 ? 4 + 4ull * ntrans : 12 + 16ull * ntrans;
-    const unsigned long long tot = ntrans > 0 ? first_ops / c0 : 0;
-    *opcnt = tot * c;
-  }
+  if (opcnt) *opcnt = total_ops;
+}
+
+// sharp_execute on host arrays: jobs of several transforms go through the
+// pipelined path; returns false (nothing done) where the plain path applies.
+bool execute_pipelined(sharp_jobtype type, int spin, void *alm, void *map,
+                       const sharp_geom_info *ginfo, const sharp_alm_info *ainfo, int ntrans,
+                       int flags, double *time, unsigned long long *opcnt) {
+  if (!pipelinable(type, spin, alm, map, ginfo, ainfo, ntrans, flags)) return false;
+  const int piece = spin > 0 ? 3 : (type == SHARP_MAP2ALM ? 6 : 4);
+  if (ntrans <= piece) return false;
+  const double t0 = wall_now();
+  execute_pipelined_jobs({HostJob{type, spin, alm, map, ginfo, ainfo, ntrans, flags}}, opcnt);
   if (time) *time = wall_now() - t0;
   return true;
 }
@@ -993,11 +1028,25 @@ int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
     g->ntrans += j.ntrans;
   }
   unsigned long long tot = 0;
-  for (auto &g : groups) {
-    unsigned long long oc = 0;
-    execute_impl(g.first->type, g.first->spin, g.alm.data(), g.map.data(), g.first->geom_info,
-                 g.first->alm_info, g.ntrans, g.first->flags, device_ptrs, stream, nullptr, &oc);
-    tot += oc;
+  // host arrays: every merged group through one pipelined sequence of pieces
+  // (one fill and one drain for the batch) where each group allows it
+  bool pipe = !device_ptrs && !groups.empty();
+  for (auto &g : groups)
+    pipe = pipe && pipelinable(g.first->type, g.first->spin, g.alm.data(), g.map.data(),
+                               g.first->geom_info, g.first->alm_info, g.ntrans, g.first->flags);
+  if (pipe) {
+    std::vector<HostJob> hj;
+    for (auto &g : groups)
+      hj.push_back(HostJob{g.first->type, g.first->spin, g.alm.data(), g.map.data(),
+                           g.first->geom_info, g.first->alm_info, g.ntrans, g.first->flags});
+    execute_pipelined_jobs(hj, &tot);
+  } else {
+    for (auto &g : groups) {
+      unsigned long long oc = 0;
+      execute_impl(g.first->type, g.first->spin, g.alm.data(), g.map.data(), g.first->geom_info,
+                   g.first->alm_info, g.ntrans, g.first->flags, device_ptrs, stream, nullptr, &oc);
+      tot += oc;
+    }
   }
   if (opcnt) *opcnt = tot;
   return int(groups.size());
