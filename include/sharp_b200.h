@@ -64,6 +64,17 @@ void sharp_b200_execute_device (sharp_jobtype type, int spin, void *alm,
    mode the failure ends the process as other errors do). */
 int sharp_b200_check_device_errors (void *stream);
 
+/* A new geometry holding the ring pairs pairs[0..npairs) of geom_info
+   (indices into geom_info->pair), the ring structs copied unchanged; free it
+   with sharp_destroy_geom_info.  It serves the decomposition of one transform
+   over several GPUs by ring pairs (each GPU runs its subset; the analysis
+   sums the partial a_lm over the GPUs), which takes the place of the
+   reference's MPI job driver sharp_execute_mpi (libsharp/sharp_mpi.h:80-83)
+   for the ring side.  Returns 0, or -1 on a bad argument (message in
+   sharp_b200_last_error()). */
+int sharp_b200_make_subset_geom_info (const sharp_geom_info *geom_info,
+  const int *pairs, int npairs, sharp_geom_info **subset);
+
 /* Drops the device tables cached for this geometry (sharp_destroy_geom_info
    calls it). */
 void sharp_b200_forget_geometry (const sharp_geom_info *geom_info);

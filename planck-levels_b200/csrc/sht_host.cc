@@ -211,6 +211,33 @@ void sharp_make_geom_info(int nrings, const int *nph, const ptrdiff_t *ofs,
 
 void sharp_b200_forget_geometry(const sharp_geom_info *info);  // device cache hook
 
+// Copies the ring pairs pairs[0..npairs) of g (indices into g->pair, in the
+// given order) into a new geometry; the ring structs are copied as they are,
+// so theta, cos/sin(theta), weights and offsets stay bit-identical.
+int sharp_b200_make_subset_geom_info(const sharp_geom_info *g, const int *pairs, int npairs,
+                                     sharp_geom_info **geom_info) {
+  if (!g || !geom_info || npairs < 0 || (npairs > 0 && !pairs)) {
+    sht::record_error("sharp_b200_make_subset_geom_info: bad argument");
+    return -1;
+  }
+  for (int i = 0; i < npairs; ++i)
+    if (pairs[i] < 0 || pairs[i] >= g->npairs) {
+      sht::record_error("sharp_b200_make_subset_geom_info: pair index out of range");
+      return -1;
+    }
+  auto *info = static_cast<sharp_geom_info *>(std::malloc(sizeof(sharp_geom_info)));
+  info->pair = static_cast<sharp_ringpair *>(
+      std::malloc(sizeof(sharp_ringpair) * std::max(npairs, 1)));
+  info->npairs = npairs;
+  info->nphmax = 0;
+  for (int i = 0; i < npairs; ++i) {
+    info->pair[i] = g->pair[pairs[i]];
+    info->nphmax = std::max(info->nphmax, std::max(info->pair[i].r1.nph, info->pair[i].r2.nph));
+  }
+  *geom_info = info;
+  return 0;
+}
+
 void sharp_destroy_geom_info(sharp_geom_info *info) {
   if (!info) return;
   sharp_b200_forget_geometry(info);

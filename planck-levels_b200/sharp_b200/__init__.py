@@ -78,6 +78,11 @@ for _nm in ("gauss", "fejer1", "fejer2", "cc", "mw"):
 _lib.sharp_make_geom_info.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, _PG]
 _lib.sharp_destroy_geom_info.argtypes = [C.POINTER(sharp_geom_info)]
+_lib.sharp_b200_make_subset_geom_info.argtypes = [C.POINTER(sharp_geom_info), C.c_void_p, C.c_int,
+                                                  _PG]
+_lib.sharp_b200_make_subset_geom_info.restype = C.c_int
+_lib.sharp_get_mlim.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double]
+_lib.sharp_get_mlim.restype = C.c_int
 _lib.sharp_make_triangular_alm_info.argtypes = [C.c_int, C.c_int, C.c_int, _PA]
 _lib.sharp_make_rectangular_alm_info.argtypes = [C.c_int, C.c_int, C.c_int, _PA]
 _lib.sharp_make_alm_info.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, _PA]
@@ -180,6 +185,16 @@ class Geometry:
     def npix(self) -> int:
         g = self.ptr.contents
         return sum(g.pair[i].r1.nph + max(g.pair[i].r2.nph, 0) for i in range(g.npairs))
+
+    def subset(self, pairs) -> "Geometry":
+        """sharp_b200_make_subset_geom_info: a geometry of the ring pairs
+        ``pairs`` (indices into this geometry's pair array)."""
+        idx = np.ascontiguousarray(pairs, np.int32)
+        p = C.POINTER(sharp_geom_info)()
+        rc = _lib.sharp_b200_make_subset_geom_info(self.ptr, idx.ctypes.data, len(idx), C.byref(p))
+        if rc != 0:
+            _check()
+        return Geometry(p)
 
     @classmethod
     def healpix(cls, nside: int, weight=None, stride: int = 1) -> "Geometry":
