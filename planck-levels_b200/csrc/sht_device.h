@@ -53,9 +53,21 @@ struct GeomHost {
   std::vector<int> blue_idx;          // descriptors that use Bluestein
   long long tw_total = 0, bhat_total = 0;
   std::vector<int> cls_N, cls_start, cls_count, cls_bufA, cls_bufB, cls_pairs;
+  // pairs whose rings run the power-of-two register FFT (pow2_ring_length):
+  // complex length pw_N[c], listed at pw_pairs[pw_start[c] .. +pw_count[c])
+  std::vector<int> pw_N, pw_start, pw_count, pw_pairs;
   long long map_lo = 0, map_hi = 0;
   bool map_covered = false;
 };
+// Complex FFT length N of a ring that the power-of-two ring kernels take
+// (n = 2N pixels with N in {1024, 2048, 4096, 8192}, unit stride, no alias
+// folding: mm <= N), else 0.
+inline int pow2_ring_length(int nph, int stride, int mm) {
+  if (nph <= 0 || (nph & 1) || stride != 1) return 0;
+  const int N = nph / 2;
+  if (N != 1024 && N != 2048 && N != 4096 && N != 8192) return 0;
+  return mm <= N ? N : 0;
+}
 GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin);
 
 // Per-geometry device tables (pairs in internal mlim order).
@@ -87,6 +99,9 @@ struct GeomPlan {
   // <= cls_N[c], listed at cls_pairs[cls_start[c] .. +cls_count[c])
   std::vector<int> cls_N, cls_start, cls_count, cls_bufA, cls_bufB;
   int *cls_pairs = nullptr;
+  // power-of-two register-FFT classes (see GeomHost)
+  std::vector<int> pw_N, pw_start, pw_count;
+  int *pw_pairs = nullptr;
   long long map_lo = 0, map_hi = 0;  // pixel index extent [lo, hi)
   bool map_covered = false;          // rings tile [lo,hi) exactly
   GeomPlan() = default;

@@ -275,10 +275,35 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
   h.map_lo = lo;
   h.map_hi = hi;
   h.map_covered = covered;
+  // pairs whose present rings all take the power-of-two register FFT with
+  // the same length run there; the rest go to the size classes
+  std::map<int, std::vector<int>> pw_lists;
+  std::vector<char> is_pw(np, 0);
+  for (int p = 0; p < np; ++p) {
+    const int mm = std::min(mmax, h.mlim_sorted[p]);
+    int N = -1;
+    for (int hh = 0; hh < 2; ++hh) {
+      const int i = 2 * p + hh;
+      if (h.nph[i] <= 0) continue;
+      const int n = pow2_ring_length(h.nph[i], h.stride[i], mm);
+      N = (N < 0 || N == n) ? n : 0;
+    }
+    if (N > 0) {
+      pw_lists[N].push_back(p);
+      is_pw[p] = 1;
+    }
+  }
+  for (auto &kv : pw_lists) {
+    h.pw_N.push_back(kv.first);
+    h.pw_start.push_back(int(h.pw_pairs.size()));
+    h.pw_count.push_back(int(kv.second.size()));
+    h.pw_pairs.insert(h.pw_pairs.end(), kv.second.begin(), kv.second.end());
+  }
   // FFT size classes (the last class is capped by shared memory)
   const int bounds[4] = {256, 1024, 4096, h.nmax_complex};
   std::vector<std::vector<int>> lists(4);
   for (int p = 0; p < np; ++p) {
+    if (is_pw[p]) continue;
     int nmx = 0;
     for (int hh = 0; hh < 2; ++hh)
       if (h.nph[2 * p + hh] > 0) nmx = std::max(nmx, h.descs[h.fft[2 * p + hh]].N);
@@ -343,6 +368,10 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   gp->map_hi = h.map_hi;
   gp->map_covered = h.map_covered;
   gp->cls_pairs = dev_upload(h.cls_pairs, st);
+  gp->pw_N = h.pw_N;
+  gp->pw_start = h.pw_start;
+  gp->pw_count = h.pw_count;
+  gp->pw_pairs = dev_upload(h.pw_pairs, st);
   gp->cth = dev_upload(h.cth, st);
   gp->sth = dev_upload(h.sth, st);
   gp->mlim = dev_upload(h.mlim_sorted, st);
@@ -1058,7 +1087,7 @@ GeomPlan::~GeomPlan() {
   dev_free(cth); dev_free(sth); dev_free(mlim); dev_free(count); dev_free(items);
   dev_free(mitems);
   dev_free(phi0); dev_free(weight); dev_free(ofs); dev_free(nph); dev_free(stride);
-  dev_free(fft); dev_free(fdesc); dev_free(twiddle); dev_free(cls_pairs);
+  dev_free(fft); dev_free(fdesc); dev_free(twiddle); dev_free(cls_pairs); dev_free(pw_pairs);
   dev_free(bhat); dev_free(wpow2);
 }
 CoefPlan::~CoefPlan() {

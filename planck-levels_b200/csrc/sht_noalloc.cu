@@ -125,6 +125,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   const size_t o_fft = L.take<int>(2 * np);
   const size_t o_fdesc = L.take<FftDesc>(h.descs.size());
   const size_t o_cls = L.take<int>(h.cls_pairs.size());
+  const size_t o_pwp = L.take<int>(h.pw_pairs.size());
   const size_t o_twn = L.take<int>(h.tw_n.size()), o_twoff = L.take<int>(h.tw_off.size());
   const size_t o_blue = L.take<int>(h.blue_idx.size());
   const size_t o_tw = L.take<double2>(h.tw_total);
@@ -164,6 +165,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   put(o_fft, h.fft.data(), sizeof(int) * 2 * np);
   put(o_fdesc, h.descs.data(), sizeof(FftDesc) * h.descs.size());
   put(o_cls, h.cls_pairs.data(), sizeof(int) * h.cls_pairs.size());
+  put(o_pwp, h.pw_pairs.data(), sizeof(int) * h.pw_pairs.size());
   put(o_twn, h.tw_n.data(), sizeof(int) * h.tw_n.size());
   put(o_twoff, h.tw_off.data(), sizeof(int) * h.tw_off.size());
   put(o_blue, h.blue_idx.data(), sizeof(int) * h.blue_idx.size());
@@ -186,6 +188,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
       g.cth = g.sth = nullptr; g.mlim = g.count = nullptr; g.items = nullptr;
       g.phi0 = g.weight = nullptr; g.ofs = nullptr; g.nph = g.stride = g.fft = nullptr;
       g.fdesc = nullptr; g.twiddle = g.bhat = g.wpow2 = nullptr; g.cls_pairs = nullptr;
+      g.pw_pairs = nullptr;
       c.d_moff = nullptr; c.alpha = c.beta = c.cfac = c.seed = nullptr; c.seed_exp = nullptr;
       a.mvstart = nullptr;
     }
@@ -205,6 +208,8 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   gp.cls_N = h.cls_N; gp.cls_start = h.cls_start; gp.cls_count = h.cls_count;
   gp.cls_bufA = h.cls_bufA; gp.cls_bufB = h.cls_bufB;
   gp.cls_pairs = static_cast<int *>(at(o_cls));
+  gp.pw_N = h.pw_N; gp.pw_start = h.pw_start; gp.pw_count = h.pw_count;
+  gp.pw_pairs = static_cast<int *>(at(o_pwp));
   cp.lmax = lmax; cp.mmax = mmax; cp.spin = 0; cp.total = off; cp.moff = moff;
   cp.d_moff = static_cast<long long *>(at(o_moff));
   cp.alpha = static_cast<double *>(at(o_alpha)); cp.cfac = static_cast<double *>(at(o_cfac));

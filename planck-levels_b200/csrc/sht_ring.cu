@@ -677,6 +677,265 @@ __global__ void __launch_bounds__(1024) ring2phase_kernel(const int *__restrict_
 }
 
 // ---------------------------------------------------------------------------
+// Power-of-two rings (n = 2N real pixels, N = 1024 .. 8192; every equatorial
+// HEALPix ring when Nside is a power of two) with no alias folding
+// (mlim <= N): one CTA per ring and component, N/16 threads holding 16
+// complex values each.  The complex FFT of length N runs as in-place
+// decimation-in-frequency passes over one shared buffer: radix-16 passes in
+// registers (a 16-point DFT as 4 x 4 with internal twiddles), then one pass
+// of radix 2, 4 or 8 for the remaining factor; the output is in digit-
+// reversed order, which the final global access undoes.  The packing of the
+// real transform (the C_k / C_{N-k} twist) is fused into the global phase
+// reads (synthesis) or the phase writes (analysis), so the buffer is read
+// and written once per pass.  Buffer entries are padded (p + p/16 + p/256)
+// so that the strided accesses of every pass spread over the bank groups.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int pw_pad(int p) { return p + (p >> 4) + (p >> 8); }
+__host__ __device__ constexpr int pw_entries(int N) {
+  return (N - 1) + ((N - 1) >> 4) + ((N - 1) >> 8) + 1;
+}
+__host__ __device__ constexpr int pw_passes16(int N) {
+  return N >= 4096 ? 3 : 2;   // 1024 = 16^2 4, 2048 = 16^2 8, 4096 = 16^3, 8192 = 16^3 2
+}
+__host__ __device__ constexpr int pw_last(int N) {
+  return N / (pw_passes16(N) == 3 ? 4096 : 256);
+}
+
+// cos(2 pi e / 16), e = 0 .. 15
+__device__ __forceinline__ double cos16(int e) {
+  switch (e & 15) {
+    case 0: return 1.0;
+    case 1: case 15: return 0.92387953251128675613;
+    case 2: case 14: return 0.70710678118654752440;
+    case 3: case 13: return 0.38268343236508977173;
+    case 4: case 12: return 0.0;
+    case 5: case 11: return -0.38268343236508977173;
+    case 6: case 10: return -0.70710678118654752440;
+    case 7: case 9: return -0.92387953251128675613;
+    default: return -1.0;
+  }
+}
+// exp(-+2 pi i e / 16) (INV: +); sin(2 pi e/16) = cos(2 pi (e - 4)/16)
+template <bool INV>
+__device__ __forceinline__ double2 w16(int e) {
+  const double sn = cos16(e + 12);
+  return make_double2(cos16(e), INV ? sn : -sn);
+}
+
+// 16-point DFT in place: v[n2 + 4 n1] -> X[k1 + 4 k2] = v[k1 + 4 k2]
+template <bool INV>
+__device__ __forceinline__ void dft16(double2 (&v)[16]) {
+  double2 y[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    double2 t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
+    small_dft<4>(t, INV);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      const int e = n2 * k1;
+      if (e == 0) y[k1][n2] = t[k1];
+      else if (e == 4) y[k1][n2] = INV ? make_double2(-t[k1].y, t[k1].x)
+                                       : make_double2(t[k1].y, -t[k1].x);
+      else y[k1][n2] = cmul(t[k1], w16<INV>(e));
+    }
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    small_dft<4>(y[k1], INV);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = y[k1][k2];
+  }
+}
+
+// One radix-16 DIF pass of length len (stride len/16) over the buffer;
+// twiddles W_len^(k0 f) from the per-length table W (exp(-2 pi i j/n),
+// n = 2N, so W_len^e = W[(2N/len) e]).
+template <int N, bool INV>
+__device__ __forceinline__ void pw_pass16(double2 *buf, int len, const double2 *__restrict__ W) {
+  const int s = len >> 4;
+  const int u = threadIdx.x;
+  const int k0 = u & (s - 1);
+  const int base = (u / s) * len + k0;
+  double2 v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = buf[pw_pad(base + s * i)];
+  dft16<INV>(v);
+  if (s > 1 && k0 > 0) {
+    double2 w1 = __ldg(W + (2 * N / len) * k0);
+    if (INV) w1.y = -w1.y;
+    double2 w = w1;
+#pragma unroll
+    for (int f = 1; f < 16; ++f) {
+      v[f] = cmul(v[f], w);
+      if (f < 15) w = cmul(w, w1);
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 16; ++f) buf[pw_pad(base + s * f)] = v[f];
+}
+
+// The last pass (radix R = 2, 4 or 8 over blocks of R, no twiddles)
+template <int N, int R, bool INV>
+__device__ __forceinline__ void pw_pass_last(double2 *buf) {
+#pragma unroll
+  for (int q = 0; q < 16 / R; ++q) {
+    const int b = threadIdx.x + (N / 16) * q;
+    double2 v[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = buf[pw_pad(b * R + i)];
+    small_dft<R>(v, INV);
+#pragma unroll
+    for (int i = 0; i < R; ++i) buf[pw_pad(b * R + i)] = v[i];
+  }
+}
+
+template <int N, bool INV>
+__device__ void pw_fft(double2 *buf, const double2 *__restrict__ W) {
+  int len = N;
+#pragma unroll
+  for (int q = 0; q < pw_passes16(N); ++q) {
+    pw_pass16<N, INV>(buf, len, W);
+    __syncthreads();
+    len >>= 4;
+  }
+  constexpr int RL = pw_last(N);
+  if constexpr (RL > 1) {
+    pw_pass_last<N, RL, INV>(buf);
+    __syncthreads();
+  }
+}
+
+// Buffer position of frequency k after pw_fft (digits reversed)
+template <int N>
+__device__ __forceinline__ int pw_pos(int k) {
+  int p = 0, rem = k, stride = N;
+#pragma unroll
+  for (int q = 0; q < pw_passes16(N); ++q) {
+    stride >>= 4;
+    p += (rem & 15) * stride;
+    rem >>= 4;
+  }
+  return p + rem;   // the last digit (radix pw_last(N)) has stride 1
+}
+
+// phase -> ring.  Grid: (2 * pairs of this length, components).
+template <typename T, int N>
+__global__ void __launch_bounds__(N / 16)
+phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
+                       const int *__restrict__ nph, const long long *__restrict__ ofs,
+                       const double *__restrict__ phi0, const double *__restrict__ weight,
+                       const int *__restrict__ fftidx, const FftDesc *__restrict__ fdesc,
+                       const double2 *__restrict__ twiddle, const double2 *__restrict__ phase,
+                       int ncm, int mmax, int flags, T *const *__restrict__ maps,
+                       long long map_lo) {
+  extern __shared__ double2 smem[];
+  double2 *buf = smem;
+  double2 *slo = smem + pw_entries(N);
+  double2 *shi = slo + kShiftLo;
+  const int p = pairs[blockIdx.x >> 1], h = blockIdx.x & 1, c = blockIdx.y;
+  const int ring = 2 * p + h;
+  if (nph[ring] <= 0) return;        // unpaired ring: nothing in this hemisphere
+  const int ms = mmax + 1;
+  const int mm = min(mmax, mlim[p]);
+  const bool add = (flags & (SHARP_ADD | SHARP_SUBTRACT)) != 0;
+  const double wgt = ((flags & SHARP_USE_WEIGHTS) ? weight[ring] : 1.0) *
+                     ((flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0) *
+                     ((flags & SHARP_SUBTRACT) ? -1.0 : 1.0);
+  const double ph = phi0[ring];
+  const bool rot = fabs(ph) >= 1e-14;
+  const double2 *W = twiddle + fdesc[fftidx[ring]].tw;
+  const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
+  if (rot) build_shift(slo, shi, mm, ph);
+  __syncthreads();
+  // t_m = phase_m wgt e^{i m phi0} (zero above mm); C_0 and C_N real
+  auto tm = [&](int m) {
+    if (m > mm) return make_double2(0.0, 0.0);
+    double2 t = cscale(src[m], wgt);
+    if (rot) t = cmul(t, shift_of(slo, shi, m));
+    return t;
+  };
+  // Z_k = (C_k + conj C_{N-k}) + i conj(W^k) (C_k - conj C_{N-k}), k < N
+#pragma unroll 4
+  for (int i = 0; i < 16; ++i) {
+    const int k = threadIdx.x + (N / 16) * i;
+    double2 ck = tm(k), cn;
+    if (k == 0) {
+      ck.y = 0.0;
+      const double2 tn = tm(N);
+      cn = make_double2(tn.x + tn.x, 0.0);   // C_N = t_N + conj t_N
+    } else {
+      cn = tm(N - k);
+    }
+    cn = cconj(cn);
+    const double2 sm = cadd(ck, cn), df = csub(ck, cn);
+    const double2 w = __ldg(W + k);
+    const double2 iw = make_double2(w.y, w.x);   // i * conj(w)
+    buf[pw_pad(k)] = cadd(sm, cmul(iw, df));
+  }
+  __syncthreads();
+  pw_fft<N, true>(buf, W);
+  // pixels 2j, 2j+1 = Re, Im z_j
+  T *map = maps[c] + (ofs[ring] - map_lo);
+#pragma unroll 4
+  for (int s2 = 0; s2 < 16; ++s2) {
+    const int j = threadIdx.x + (N / 16) * s2;
+    const double2 z = buf[pw_pad(pw_pos<N>(j))];
+    store_px(map + 2 * j, z.x, add);
+    store_px(map + 2 * j + 1, z.y, add);
+  }
+}
+
+// ring -> phase
+template <typename T, int N>
+__global__ void __launch_bounds__(N / 16)
+ring2phase_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
+                       const int *__restrict__ nph, const long long *__restrict__ ofs,
+                       const double *__restrict__ phi0, const double *__restrict__ weight,
+                       const int *__restrict__ fftidx, const FftDesc *__restrict__ fdesc,
+                       const double2 *__restrict__ twiddle, double2 *__restrict__ phase,
+                       int ncm, int mmax, int flags, const T *const *__restrict__ maps,
+                       long long map_lo) {
+  extern __shared__ double2 smem[];
+  double2 *buf = smem;
+  double2 *slo = smem + pw_entries(N);
+  double2 *shi = slo + kShiftLo;
+  const int p = pairs[blockIdx.x >> 1], h = blockIdx.x & 1, c = blockIdx.y;
+  const int ring = 2 * p + h;
+  if (nph[ring] <= 0) return;
+  const int ms = mmax + 1;
+  const int mm = min(mmax, mlim[p]);
+  const double wgt = ((flags & SHARP_USE_WEIGHTS) ? weight[ring] : 1.0) *
+                     ((flags & SHARP_REAL_HARMONICS) ? kSqrtTwo : 1.0);
+  const double ph = phi0[ring];
+  const bool rot = fabs(ph) >= 1e-14;
+  const double2 *W = twiddle + fdesc[fftidx[ring]].tw;
+  const T *map = maps[c] + (ofs[ring] - map_lo);
+  if (rot) build_shift(slo, shi, mm, -ph);
+#pragma unroll 4
+  for (int s2 = 0; s2 < 16; ++s2) {
+    const int j = threadIdx.x + (N / 16) * s2;
+    buf[pw_pad(j)] = make_double2(double(map[2 * j]), double(map[2 * j + 1]));
+  }
+  __syncthreads();
+  pw_fft<N, false>(buf, W);
+  // X_k = (Z_k + conj Z_{N-k})/2 - i W^k (Z_k - conj Z_{N-k})/2, k <= N;
+  // phase_m = X_m wgt e^{-i m phi0} for m <= mm (<= N: no folding)
+  double2 *dst = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
+  for (int k = threadIdx.x; k <= mm; k += N / 16) {
+    const double2 zk = buf[pw_pad(pw_pos<N>(k == N ? 0 : k))];
+    const double2 zn = cconj(buf[pw_pad(pw_pos<N>(k == 0 ? 0 : N - k))]);
+    const double2 sm = cadd(zk, zn), df = csub(zk, zn);
+    const double2 w = __ldg(W + k);
+    const double2 mi_w = make_double2(w.y, -w.x);  // -i * w
+    double2 xk = cscale(cadd(sm, cmul(mi_w, df)), 0.5);
+    if (k == 0 || k == N) xk.y = 0.0;
+    double2 v = cscale(xk, wgt);
+    if (rot) v = cmul(v, shift_of(slo, shi, k));
+    dst[k] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // SHARP_NO_FFT: map entries are the complex phases themselves
 // (libsharp/sharp.c:631-669); nph must equal mmax+1.
 // ---------------------------------------------------------------------------
@@ -975,10 +1234,80 @@ void ring2phase_class(const JobDesc &job, const GeomPlan &gp, int cls, long long
 
 }  // namespace
 
+namespace {
+
+size_t pow2_smem(int N, int mmax) {
+  return sizeof(double2) * (size_t(pw_entries(N)) + kShiftLo + mmax / kShiftLo + 2);
+}
+
+template <typename T, int N>
+void phase2ring_pow2(const JobDesc &job, const GeomPlan &gp, int cls, long long map_lo,
+                     const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                     cudaStream_t st) {
+  auto k = phase2ring_pow2_kernel<T, N>;
+  const size_t smem = pow2_smem(N, job.mmax);
+  SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  k<<<dim3(2 * gp.pw_count[cls], nmapptr), N / 16, smem, st>>>(
+      gp.pw_pairs + gp.pw_start[cls], gp.mlim, gp.nph, gp.ofs, gp.phi0, gp.weight, gp.fft,
+      gp.fdesc, gp.twiddle, phase, ncm, job.mmax, job.flags,
+      reinterpret_cast<T *const *>(maps_dev), map_lo);
+  SHT_CUDA(cudaGetLastError());
+}
+
+template <typename T, int N>
+void ring2phase_pow2(const JobDesc &job, const GeomPlan &gp, int cls, long long map_lo,
+                     const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
+                     cudaStream_t st) {
+  auto k = ring2phase_pow2_kernel<T, N>;
+  const size_t smem = pow2_smem(N, job.mmax);
+  SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  k<<<dim3(2 * gp.pw_count[cls], nmapptr), N / 16, smem, st>>>(
+      gp.pw_pairs + gp.pw_start[cls], gp.mlim, gp.nph, gp.ofs, gp.phi0, gp.weight, gp.fft,
+      gp.fdesc, gp.twiddle, phase, ncm, job.mmax, job.flags,
+      reinterpret_cast<const T *const *>(maps_dev), map_lo);
+  SHT_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void phase2ring_pow2_classes(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                             const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                             cudaStream_t st) {
+  for (int c = 0; c < int(gp.pw_N.size()); ++c) {
+    if (gp.pw_count[c] == 0) continue;
+    switch (gp.pw_N[c]) {
+      case 1024: phase2ring_pow2<T, 1024>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+      case 2048: phase2ring_pow2<T, 2048>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+      case 4096: phase2ring_pow2<T, 4096>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+      default: phase2ring_pow2<T, 8192>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+    }
+  }
+}
+
+template <typename T>
+void ring2phase_pow2_classes(const JobDesc &job, const GeomPlan &gp, long long map_lo,
+                             const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
+                             cudaStream_t st) {
+  for (int c = 0; c < int(gp.pw_N.size()); ++c) {
+    if (gp.pw_count[c] == 0) continue;
+    switch (gp.pw_N[c]) {
+      case 1024: ring2phase_pow2<T, 1024>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+      case 2048: ring2phase_pow2<T, 2048>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+      case 4096: ring2phase_pow2<T, 4096>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+      default: ring2phase_pow2<T, 8192>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+    }
+  }
+}
+
+}  // namespace
+
 void launch_phase2ring(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                        const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
                        cudaStream_t st) {
   ProfScope ps("ring_synth", st);
+  if (job.dp)
+    phase2ring_pow2_classes<double>(job, gp, map_lo, phase, ncm, maps_dev, nmapptr, st);
+  else
+    phase2ring_pow2_classes<float>(job, gp, map_lo, phase, ncm, maps_dev, nmapptr, st);
   for (int cls = 0; cls < int(gp.cls_N.size()); ++cls) {
     if (gp.cls_count[cls] == 0) continue;
     if (job.dp)
@@ -992,6 +1321,10 @@ void launch_ring2phase(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                        const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
                        cudaStream_t st) {
   ProfScope ps("ring_anal", st);
+  if (job.dp)
+    ring2phase_pow2_classes<double>(job, gp, map_lo, maps_dev, nmapptr, phase, ncm, st);
+  else
+    ring2phase_pow2_classes<float>(job, gp, map_lo, maps_dev, nmapptr, phase, ncm, st);
   for (int cls = 0; cls < int(gp.cls_N.size()); ++cls) {
     if (gp.cls_count[cls] == 0) continue;
     if (job.dp)
