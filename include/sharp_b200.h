@@ -121,12 +121,16 @@ typedef struct {
    No counterpart in the reference, whose callers loop over sharp_execute.
    Jobs that share type, spin, flags and the same geom_info and alm_info
    objects are merged into one job of up to 100 transforms, so the batched
-   kernels (SHARP_MIXED) see them together; merged groups run in order of
-   first appearance on one stream.  Every output equals that of
-   sharp_execute on its own job (the merge changes no arithmetic).  Jobs
-   must not share output arrays.  device_ptrs = 0: host arrays, returns
-   after the results are copied back; 1: device arrays, work enqueued on
-   `stream` as sharp_b200_execute_device.  opcnt (if non-NULL) receives the
+   kernels (SHARP_MIXED) see them together.  Every output equals that of
+   sharp_execute on its own job (neither the merge nor the scheduling
+   changes any arithmetic).  Jobs must not share output arrays.
+   device_ptrs = 0: host arrays; all merged jobs run as one pipelined
+   sequence of pieces (host->device copies, compute and device->host copies
+   overlapped across the whole batch); returns after the results are copied
+   back.  device_ptrs = 1: device arrays; the merged jobs run side by side on
+   up to four library streams forked from `stream` and joined back to it
+   (work ordered after what `stream` holds, later work on `stream` after the
+   batch), without host synchronisation.  opcnt (if non-NULL) receives the
    summed operation count.  Returns the number of merged groups executed,
    or -1 after a failure in non-abort mode. */
 int sharp_b200_execute_batch (const sharp_b200_job *jobs, int njobs,

@@ -32,7 +32,10 @@ struct FftDesc {
   int rad[kMaxRadices];
   int blue;     // 1: Bluestein convolution of power-of-two length M
   int M;
-  long long bhat;  // offset of the transformed chirp (digit order of the DIF stages, /M)
+  long long bhat;   // offset of the transformed chirp in the digit order of the
+                    // radix-4 stages (/M), or -1 when no generic-class ring uses it
+  long long bhat2;  // the same in the digit order of the radix-16 register passes,
+                    // or -1 when no register-Bluestein ring uses it
 };
 
 // Host half of a geometry plan (build_geom_host, no device calls): what the
@@ -50,15 +53,26 @@ struct GeomHost {
   std::vector<long long> ofs;
   std::vector<FftDesc> descs;
   std::vector<int> tw_n, tw_off;      // per distinct length: n and table offset
-  std::vector<int> blue_idx;          // descriptors that use Bluestein
+  std::vector<int> blue_idx;          // descriptors with a radix-4 chirp transform (bhat)
+  std::vector<int> blue2_idx;         // descriptors with a register-pass one (bhat2)
   long long tw_total = 0, bhat_total = 0;
   std::vector<int> cls_N, cls_start, cls_count, cls_bufA, cls_bufB, cls_pairs;
   // pairs whose rings run the power-of-two register FFT (pow2_ring_length):
   // complex length pw_N[c], listed at pw_pairs[pw_start[c] .. +pw_count[c])
   std::vector<int> pw_N, pw_start, pw_count, pw_pairs;
+  // pairs whose rings run the register Bluestein convolution
+  // (blue_ring_length): length pb_M[c], listed at pb_pairs[pb_start[c] ..)
+  std::vector<int> pb_M, pb_start, pb_count, pb_pairs;
   long long map_lo = 0, map_hi = 0;
   bool map_covered = false;
 };
+// Shared memory of the register ring kernels (pw_entries(N) buffer entries
+// of the ring kernels plus the phi0 rotation slices), in double2 entries.
+inline size_t pow2_ring_smem_entries(int N, int mmax) {
+  const int n = N - 1;
+  return size_t(n + (n >> 4) + (n >> 8) + 1) + 64 + mmax / 64 + 2;
+}
+constexpr size_t kRingSmemLimit = 227 * 1024;
 // Complex FFT length N of a ring that the power-of-two ring kernels take
 // (n = 2N pixels with N in {1024, 2048, 4096, 8192}, unit stride, no alias
 // folding: mm <= N), else 0.
@@ -67,6 +81,13 @@ inline int pow2_ring_length(int nph, int stride, int mm) {
   const int N = nph / 2;
   if (N != 1024 && N != 2048 && N != 4096 && N != 8192) return 0;
   return mm <= N ? N : 0;
+}
+// Convolution length M of a ring that the register Bluestein kernels take
+// (even nph whose complex length uses the Bluestein convolution with M in
+// {1024, 2048, 4096, 8192}; any stride, any alias folding), else 0.
+inline int blue_ring_length(int nph, const FftDesc &d) {
+  if (nph <= 0 || (nph & 1) || !d.blue) return 0;
+  return (d.M == 1024 || d.M == 2048 || d.M == 4096 || d.M == 8192) ? d.M : 0;
 }
 GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin);
 
@@ -102,6 +123,9 @@ struct GeomPlan {
   // power-of-two register-FFT classes (see GeomHost)
   std::vector<int> pw_N, pw_start, pw_count;
   int *pw_pairs = nullptr;
+  // register-Bluestein classes (see GeomHost)
+  std::vector<int> pb_M, pb_start, pb_count;
+  int *pb_pairs = nullptr;
   long long map_lo = 0, map_hi = 0;  // pixel index extent [lo, hi)
   bool map_covered = false;          // rings tile [lo,hi) exactly
   GeomPlan() = default;
@@ -176,11 +200,11 @@ void launch_legendre_anal(const JobDesc &job, const GeomPlan &gp, const CoefPlan
 // Ring FFT and staging launchers (sht_ring.cu)
 void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
                      const std::vector<int> &tw_off, cudaStream_t st);
-void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cudaStream_t st);
+void launch_bluestein_setup(GeomPlan &gp, const GeomHost &h, cudaStream_t st);
 void launch_twiddles_preplaced(double2 *tw, const int *d_n, const int *d_off, int ntab,
                                cudaStream_t st);
 void launch_bluestein_setup_preplaced(const GeomPlan &gp, const int *d_blue_idx, int nblue,
-                                      cudaStream_t st);
+                                      const int *d_blue2_idx, int nblue2, cudaStream_t st);
 // map_lo / alm_lo: index (in elements of the user array) that the device
 // pointers in maps_dev / alm_dev point at (0 when they are the user's own
 // device arrays, the extent start when they are staged copies).

@@ -234,7 +234,7 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
         const long long blue_cost = 2ll * ((long long)M * lg + 2ll * d.N);
         d.blue = (d.N > 16 && blue_cost < direct) ? 1 : 0;
         d.M = d.blue ? M : 0;
-        d.bhat = 0;
+        d.bhat = d.bhat2 = -1;
         h.tw_n.push_back(d.n);
         h.tw_off.push_back(int(h.tw_total));
         h.tw_total += d.n;
@@ -253,14 +253,8 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
     }
   }
   SHT_REQUIRE(h.tw_total < (1ll << 31), "geometry too large (twiddle table)");
-  for (int i = 0; i < int(h.descs.size()); ++i) {
-    FftDesc &d = h.descs[i];
-    if (!d.blue) continue;
-    d.bhat = h.bhat_total;
-    h.bhat_total += d.M;
-    h.P = std::max(h.P, d.M);
-    h.blue_idx.push_back(i);
-  }
+  for (const FftDesc &d : h.descs)
+    if (d.blue) h.P = std::max(h.P, d.M);
   // rings tile [lo,hi) exactly -> synthesis need not pre-load the map
   bool covered = unit_stride && !spans.empty();
   if (covered) {
@@ -277,19 +271,30 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
   h.map_covered = covered;
   // pairs whose present rings all take the power-of-two register FFT with
   // the same length run there; the rest go to the size classes
-  std::map<int, std::vector<int>> pw_lists;
+  // (the same for the register Bluestein kernels, keyed by the convolution
+  // length); a length whose buffer and phi0 slices exceed the shared memory
+  // of a CTA stays in the size classes
+  std::map<int, std::vector<int>> pw_lists, pb_lists;
   std::vector<char> is_pw(np, 0);
+  auto fits = [&](int len) {
+    return sizeof(double2) * pow2_ring_smem_entries(len, mmax) <= kRingSmemLimit;
+  };
   for (int p = 0; p < np; ++p) {
     const int mm = std::min(mmax, h.mlim_sorted[p]);
-    int N = -1;
+    int N = -1, M = -1;
     for (int hh = 0; hh < 2; ++hh) {
       const int i = 2 * p + hh;
       if (h.nph[i] <= 0) continue;
       const int n = pow2_ring_length(h.nph[i], h.stride[i], mm);
       N = (N < 0 || N == n) ? n : 0;
+      const int b = blue_ring_length(h.nph[i], h.descs[h.fft[i]]);
+      M = (M < 0 || M == b) ? b : 0;
     }
-    if (N > 0) {
+    if (N > 0 && fits(N)) {
       pw_lists[N].push_back(p);
+      is_pw[p] = 1;
+    } else if (M > 0 && fits(M)) {
+      pb_lists[M].push_back(p);
       is_pw[p] = 1;
     }
   }
@@ -298,6 +303,12 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
     h.pw_start.push_back(int(h.pw_pairs.size()));
     h.pw_count.push_back(int(kv.second.size()));
     h.pw_pairs.insert(h.pw_pairs.end(), kv.second.begin(), kv.second.end());
+  }
+  for (auto &kv : pb_lists) {
+    h.pb_M.push_back(kv.first);
+    h.pb_start.push_back(int(h.pb_pairs.size()));
+    h.pb_count.push_back(int(kv.second.size()));
+    h.pb_pairs.insert(h.pb_pairs.end(), kv.second.begin(), kv.second.end());
   }
   // FFT size classes (the last class is capped by shared memory)
   const int bounds[4] = {256, 1024, 4096, h.nmax_complex};
@@ -332,6 +343,28 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
     h.cls_count.push_back(int(lists[c].size()));
     h.cls_pairs.insert(h.cls_pairs.end(), lists[c].begin(), lists[c].end());
     // classes whose buffers exceed shared memory run them in global scratch
+  }
+  // chirp transforms: the radix-4 order for Bluestein rings of the size
+  // classes, the register-pass order for those of the register classes
+  std::vector<char> use4(h.descs.size(), 0), use16(h.descs.size(), 0);
+  for (int p = 0; p < np; ++p)
+    for (int hh = 0; hh < 2; ++hh) {
+      const int i = 2 * p + hh;
+      if (h.nph[i] <= 0 || !h.descs[h.fft[i]].blue) continue;
+      (is_pw[p] ? use16 : use4)[h.fft[i]] = 1;
+    }
+  for (int i = 0; i < int(h.descs.size()); ++i) {
+    FftDesc &d = h.descs[i];
+    if (use4[i]) {
+      d.bhat = h.bhat_total;
+      h.bhat_total += d.M;
+      h.blue_idx.push_back(i);
+    }
+    if (use16[i]) {
+      d.bhat2 = h.bhat_total;
+      h.bhat_total += d.M;
+      h.blue2_idx.push_back(i);
+    }
   }
   return h;
 }
@@ -372,6 +405,10 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   gp->pw_start = h.pw_start;
   gp->pw_count = h.pw_count;
   gp->pw_pairs = dev_upload(h.pw_pairs, st);
+  gp->pb_M = h.pb_M;
+  gp->pb_start = h.pb_start;
+  gp->pb_count = h.pb_count;
+  gp->pb_pairs = dev_upload(h.pb_pairs, st);
   gp->cth = dev_upload(h.cth, st);
   gp->sth = dev_upload(h.sth, st);
   gp->mlim = dev_upload(h.mlim_sorted, st);
@@ -389,7 +426,7 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   launch_twiddles(*gp, int(h.tw_total), h.tw_n, h.tw_off, st);
   SHT_CUDA(cudaMalloc(&gp->bhat, sizeof(double2) * std::max<long long>(h.bhat_total, 1)));
   SHT_CUDA(cudaMalloc(&gp->wpow2, sizeof(double2) * gp->P));
-  launch_bluestein_setup(*gp, h.descs, st);
+  launch_bluestein_setup(*gp, h, st);
   SHT_CUDA(cudaStreamSynchronize(st));
   return gp;
 }
@@ -823,8 +860,12 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
 // transform's arithmetic is that of the single-call path, so the results
 // are the same.  Returns false (nothing done) where the plain path applies.
 // ---------------------------------------------------------------------------
+// Library streams of the current device: 0 and 1 carry the host-array
+// copies, 2 .. 2 + kBatchLanes - 1 the concurrent groups of a batch.
 cudaStream_t copy_stream(int which) {
   static std::map<std::pair<int, int>, cudaStream_t> streams;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
   int dev = 0;
   SHT_CUDA(cudaGetDevice(&dev));
   auto key = std::make_pair(dev, which);
@@ -1069,6 +1110,55 @@ int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
       hj.push_back(HostJob{g.first->type, g.first->spin, g.alm.data(), g.map.data(),
                            g.first->geom_info, g.first->alm_info, g.ntrans, g.first->flags});
     execute_pipelined_jobs(hj, &tot);
+  } else if (device_ptrs && groups.size() > 1) {
+    // device arrays: the merged groups run side by side on up to kBatchLanes
+    // library streams (forked from and joined back to the caller's stream),
+    // so groups of uneven size fill the GPU together; largest groups first,
+    // each to the least loaded lane.  The groups write disjoint outputs.
+    constexpr int kBatchLanes = 4;
+    const int lanes = std::min<int>(kBatchLanes, int(groups.size()));
+    std::vector<int> order(groups.size());
+    std::iota(order.begin(), order.end(), 0);
+    auto cost = [&](int i) {
+      const sharp_b200_job &f = *groups[i].first;
+      const double l1 = f.alm_info->lmax + 1.0;
+      return double(groups[i].ntrans) * l1 * l1 * (f.spin > 0 ? 3.0 : 1.0);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<double> load(lanes, 0.0);
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join(lanes, nullptr);
+    SHT_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    for (auto &e : join) SHT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    SHT_CUDA(cudaEventRecord(fork, stream));
+    for (int i = 0; i < lanes; ++i) SHT_CUDA(cudaStreamWaitEvent(copy_stream(2 + i), fork, 0));
+    try {
+      for (int gi : order) {
+        const int lane = int(std::min_element(load.begin(), load.end()) - load.begin());
+        load[lane] += cost(gi);
+        Group &g = groups[gi];
+        unsigned long long oc = 0;
+        execute_impl(g.first->type, g.first->spin, g.alm.data(), g.map.data(),
+                     g.first->geom_info, g.first->alm_info, g.ntrans, g.first->flags, true,
+                     copy_stream(2 + lane), nullptr, &oc);
+        tot += oc;
+      }
+    } catch (const Failure &) {
+      // join what was enqueued before reporting
+      for (int i = 0; i < lanes; ++i) {
+        cudaEventRecord(join[i], copy_stream(2 + i));
+        cudaStreamWaitEvent(stream, join[i], 0);
+      }
+      cudaEventDestroy(fork);
+      for (auto &e : join) cudaEventDestroy(e);
+      throw;
+    }
+    for (int i = 0; i < lanes; ++i) {
+      SHT_CUDA(cudaEventRecord(join[i], copy_stream(2 + i)));
+      SHT_CUDA(cudaStreamWaitEvent(stream, join[i], 0));
+    }
+    SHT_CUDA(cudaEventDestroy(fork));
+    for (auto &e : join) SHT_CUDA(cudaEventDestroy(e));
   } else {
     for (auto &g : groups) {
       unsigned long long oc = 0;
@@ -1088,6 +1178,7 @@ GeomPlan::~GeomPlan() {
   dev_free(mitems);
   dev_free(phi0); dev_free(weight); dev_free(ofs); dev_free(nph); dev_free(stride);
   dev_free(fft); dev_free(fdesc); dev_free(twiddle); dev_free(cls_pairs); dev_free(pw_pairs);
+  dev_free(pb_pairs);
   dev_free(bhat); dev_free(wpow2);
 }
 CoefPlan::~CoefPlan() {

@@ -128,6 +128,8 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   const size_t o_pwp = L.take<int>(h.pw_pairs.size());
   const size_t o_twn = L.take<int>(h.tw_n.size()), o_twoff = L.take<int>(h.tw_off.size());
   const size_t o_blue = L.take<int>(h.blue_idx.size());
+  const size_t o_blue2 = L.take<int>(h.blue2_idx.size());
+  const size_t o_pbp = L.take<int>(h.pb_pairs.size());
   const size_t o_tw = L.take<double2>(h.tw_total);
   const size_t o_wp = L.take<double2>(h.P);
   const size_t o_bhat = L.take<double2>(h.bhat_total);
@@ -169,6 +171,8 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   put(o_twn, h.tw_n.data(), sizeof(int) * h.tw_n.size());
   put(o_twoff, h.tw_off.data(), sizeof(int) * h.tw_off.size());
   put(o_blue, h.blue_idx.data(), sizeof(int) * h.blue_idx.size());
+  put(o_blue2, h.blue2_idx.data(), sizeof(int) * h.blue2_idx.size());
+  put(o_pbp, h.pb_pairs.data(), sizeof(int) * h.pb_pairs.size());
   put(o_moff, moff.data(), sizeof(long long) * (mmax + 2));
   put(o_mfac, mfac.data(), sizeof(double) * (mmax + 1));
   put(o_mvs, mvstart.data(), sizeof(long long) * (mmax + 1));
@@ -188,7 +192,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
       g.cth = g.sth = nullptr; g.mlim = g.count = nullptr; g.items = nullptr;
       g.phi0 = g.weight = nullptr; g.ofs = nullptr; g.nph = g.stride = g.fft = nullptr;
       g.fdesc = nullptr; g.twiddle = g.bhat = g.wpow2 = nullptr; g.cls_pairs = nullptr;
-      g.pw_pairs = nullptr;
+      g.pw_pairs = nullptr; g.pb_pairs = nullptr;
       c.d_moff = nullptr; c.alpha = c.beta = c.cfac = c.seed = nullptr; c.seed_exp = nullptr;
       a.mvstart = nullptr;
     }
@@ -210,6 +214,8 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   gp.cls_pairs = static_cast<int *>(at(o_cls));
   gp.pw_N = h.pw_N; gp.pw_start = h.pw_start; gp.pw_count = h.pw_count;
   gp.pw_pairs = static_cast<int *>(at(o_pwp));
+  gp.pb_M = h.pb_M; gp.pb_start = h.pb_start; gp.pb_count = h.pb_count;
+  gp.pb_pairs = static_cast<int *>(at(o_pbp));
   cp.lmax = lmax; cp.mmax = mmax; cp.spin = 0; cp.total = off; cp.moff = moff;
   cp.d_moff = static_cast<long long *>(at(o_moff));
   cp.alpha = static_cast<double *>(at(o_alpha)); cp.cfac = static_cast<double *>(at(o_cfac));
@@ -230,6 +236,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   launch_twiddles_preplaced(gp.wpow2, static_cast<int *>(at(o_pw)),
                             static_cast<int *>(at(o_pw)) + 1, 1, st);
   launch_bluestein_setup_preplaced(gp, static_cast<int *>(at(o_blue)), int(h.blue_idx.size()),
+                                   static_cast<int *>(at(o_blue2)), int(h.blue2_idx.size()),
                                    st);
   launch_coef_tables(cp, st);
   auto *ptr_dev = static_cast<void *const *>(at(o_ptr));

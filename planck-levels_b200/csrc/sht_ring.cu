@@ -748,20 +748,23 @@ __device__ __forceinline__ void dft16(double2 (&v)[16]) {
 }
 
 // One radix-16 DIF pass of length len (stride len/16) over the buffer;
-// twiddles W_len^(k0 f) from the per-length table W (exp(-2 pi i j/n),
-// n = 2N, so W_len^e = W[(2N/len) e]).
-template <int N, bool INV>
-__device__ __forceinline__ void pw_pass16(double2 *buf, int len, const double2 *__restrict__ W) {
+// twiddles W_len^(k0 f) from a table W of exp(-2 pi i j/tl), j < tl (a
+// multiple of len), so W_len^e = W[(tl/len) e].
+// Inputs i >= NIN are taken as zero (not read).
+template <int N, bool INV, int NIN = 16>
+__device__ __forceinline__ void pw_pass16(double2 *buf, int len, const double2 *__restrict__ W,
+                                          int tl) {
   const int s = len >> 4;
   const int u = threadIdx.x;
   const int k0 = u & (s - 1);
   const int base = (u / s) * len + k0;
   double2 v[16];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = buf[pw_pad(base + s * i)];
+  for (int i = 0; i < 16; ++i)
+    v[i] = i < NIN ? buf[pw_pad(base + s * i)] : make_double2(0.0, 0.0);
   dft16<INV>(v);
   if (s > 1 && k0 > 0) {
-    double2 w1 = __ldg(W + (2 * N / len) * k0);
+    double2 w1 = __ldg(W + (tl / len) * k0);
     if (INV) w1.y = -w1.y;
     double2 w = w1;
 #pragma unroll
@@ -790,11 +793,11 @@ __device__ __forceinline__ void pw_pass_last(double2 *buf) {
 }
 
 template <int N, bool INV>
-__device__ void pw_fft(double2 *buf, const double2 *__restrict__ W) {
+__device__ void pw_fft(double2 *buf, const double2 *__restrict__ W, int tl) {
   int len = N;
 #pragma unroll
   for (int q = 0; q < pw_passes16(N); ++q) {
-    pw_pass16<N, INV>(buf, len, W);
+    pw_pass16<N, INV>(buf, len, W, tl);
     __syncthreads();
     len >>= 4;
   }
@@ -803,6 +806,37 @@ __device__ void pw_fft(double2 *buf, const double2 *__restrict__ W) {
     pw_pass_last<N, RL, INV>(buf);
     __syncthreads();
   }
+}
+
+// The transposed pass of pw_pass16 with the opposite sign: inputs at the
+// positions pw_pass16 writes, times conj(W_len^(k0 f)), then the 16-point
+// DFT with positive sign.  Run in the reverse order of the passes of
+// pw_fft<N, false>, the chain maps its digit-reversed output back to
+// natural order and computes the unnormalised inverse DFT.  Outputs
+// i >= NOUT are not stored.
+template <int N, int NOUT = 16>
+__device__ __forceinline__ void pw_pass16_back(double2 *buf, int len,
+                                               const double2 *__restrict__ W, int tl) {
+  const int s = len >> 4;
+  const int u = threadIdx.x;
+  const int k0 = u & (s - 1);
+  const int base = (u / s) * len + k0;
+  double2 v[16];
+#pragma unroll
+  for (int f = 0; f < 16; ++f) v[f] = buf[pw_pad(base + s * f)];
+  if (s > 1 && k0 > 0) {
+    double2 w1 = __ldg(W + (tl / len) * k0);
+    w1.y = -w1.y;
+    double2 w = w1;
+#pragma unroll
+    for (int f = 1; f < 16; ++f) {
+      v[f] = cmul(v[f], w);
+      if (f < 15) w = cmul(w, w1);
+    }
+  }
+  dft16<true>(v);
+#pragma unroll
+  for (int i = 0; i < NOUT; ++i) buf[pw_pad(base + s * i)] = v[i];
 }
 
 // Buffer position of frequency k after pw_fft (digits reversed)
@@ -873,7 +907,7 @@ phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     buf[pw_pad(k)] = cadd(sm, cmul(iw, df));
   }
   __syncthreads();
-  pw_fft<N, true>(buf, W);
+  pw_fft<N, true>(buf, W, 2 * N);
   // pixels 2j, 2j+1 = Re, Im z_j
   T *map = maps[c] + (ofs[ring] - map_lo);
 #pragma unroll 4
@@ -917,7 +951,7 @@ ring2phase_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     buf[pw_pad(j)] = make_double2(double(map[2 * j]), double(map[2 * j + 1]));
   }
   __syncthreads();
-  pw_fft<N, false>(buf, W);
+  pw_fft<N, false>(buf, W, 2 * N);
   // X_k = (Z_k + conj Z_{N-k})/2 - i W^k (Z_k - conj Z_{N-k})/2, k <= N;
   // phase_m = X_m wgt e^{-i m phi0} for m <= mm (<= N: no folding)
   double2 *dst = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
@@ -932,6 +966,263 @@ ring2phase_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     double2 v = cscale(xk, wgt);
     if (rot) v = cmul(v, shift_of(slo, shi, k));
     dst[k] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bluestein rings in registers: even rings n = 2N whose complex length N
+// takes the Bluestein convolution with M in {1024, 2048, 4096, 8192} (the
+// polar HEALPix rings nph = 4i whose i has a large prime factor), with any
+// stride and any alias folding.  One CTA per ring and component, M/16
+// threads.  The convolution reuses the radix-16 passes of the power-of-two
+// rings over one padded shared buffer:
+//  * forward passes over x_j c_j, c_j = exp(-pi i j^2/N), whose upper half
+//    (j >= M/2 >= N) is the zero padding and is not read;
+//  * the product with the chirp spectrum (DFT of b_j = conj c_j, |j| < N,
+//    scaled by 1/M and stored in the passes' digit order) fused between the
+//    last forward pass and the first transposed one, which act on the same
+//    registers;
+//  * the transposed passes back to natural order; of the last only the
+//    lower half (the outputs k < N) is stored.
+// X_k = c_k (x c * b)_k; the inverse transform is conj(forward(conj x)).
+// The alias folding and the real-FFT twist run in the same buffer around
+// the convolution, pairing k with N-k so that each thread updates its own
+// entries in place.
+// ---------------------------------------------------------------------------
+// c_j from the ring's table exp(-2 pi i e/n): c_j = W[j^2 mod n] (n = 2N)
+__device__ __forceinline__ double2 pb_chirp(const double2 *__restrict__ W, int j, int n) {
+  return __ldg(W + int((unsigned(j) * unsigned(j)) % unsigned(n)));
+}
+
+// In place: natural-order input (upper half zero) -> M times the cyclic
+// convolution with b, natural order, lower half.  W: exp(-2 pi i j/tl).
+template <int M>
+__device__ void pb_convolve(double2 *buf, const double2 *__restrict__ W, int tl,
+                            const double2 *__restrict__ bh) {
+  constexpr int P16 = pw_passes16(M), RL = pw_last(M);
+  constexpr int FWD = (RL > 1) ? P16 : P16 - 1;   // radix-16 passes before the product
+  int len = M;
+#pragma unroll
+  for (int q = 0; q < FWD; ++q) {
+    if (q == 0) pw_pass16<M, false, 8>(buf, len, W, tl);
+    else pw_pass16<M, false>(buf, len, W, tl);
+    __syncthreads();
+    len >>= 4;
+  }
+  if constexpr (RL > 1) {
+    // last forward pass (radix RL, unit twiddles), product, its inverse
+#pragma unroll
+    for (int q = 0; q < 16 / RL; ++q) {
+      const int b = threadIdx.x + (M / 16) * q;
+      double2 v[RL];
+#pragma unroll
+      for (int i = 0; i < RL; ++i) v[i] = buf[pw_pad(b * RL + i)];
+      small_dft<RL>(v, false);
+#pragma unroll
+      for (int i = 0; i < RL; ++i) v[i] = cmul(v[i], __ldg(bh + b * RL + i));
+      small_dft<RL>(v, true);
+#pragma unroll
+      for (int i = 0; i < RL; ++i) buf[pw_pad(b * RL + i)] = v[i];
+    }
+  } else {
+    // the radix-16 pass of length 16 (unit twiddles), product, its inverse
+    const int b = threadIdx.x * 16;
+    double2 v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = buf[pw_pad(b + i)];
+    dft16<false>(v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = cmul(v[i], __ldg(bh + b + i));
+    dft16<true>(v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) buf[pw_pad(b + i)] = v[i];
+  }
+  __syncthreads();
+  len = (RL > 1) ? 16 * RL : 256;
+#pragma unroll
+  for (int q = 0; q < FWD; ++q) {
+    if (q == FWD - 1) pw_pass16_back<M, 8>(buf, len, W, tl);
+    else pw_pass16_back<M>(buf, len, W, tl);
+    __syncthreads();
+    len <<= 4;
+  }
+}
+
+// Chirp spectra in the digit order of the register passes: one CTA per
+// descriptor of blue2 (those of other lengths return at once).
+template <int M>
+__global__ void __launch_bounds__(M / 16)
+bluestein_pw_setup_kernel(const FftDesc *__restrict__ fdesc, const int *__restrict__ blue2_idx,
+                          const double2 *__restrict__ twiddle,
+                          const double2 *__restrict__ wpow2, int P,
+                          double2 *__restrict__ bhat) {
+  extern __shared__ double2 smem[];
+  const FftDesc &d = fdesc[blue2_idx[blockIdx.x]];
+  if (d.M != M) return;
+  const int N = d.N, n = d.n;
+  const long long o = d.bhat2;
+  const double2 *W = twiddle + d.tw;
+  for (int j = threadIdx.x; j < M; j += M / 16) {
+    const int jj = j < N ? j : (j > M - N ? M - j : -1);
+    smem[pw_pad(j)] = jj >= 0 ? cconj(pb_chirp(W, jj, n)) : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  pw_fft<M, false>(smem, wpow2, P);
+  for (int j = threadIdx.x; j < M; j += M / 16)
+    bhat[o + j] = cscale(smem[pw_pad(j)], 1.0 / M);
+}
+
+// phase -> ring.  Grid: (2 * pairs of this length, components).
+template <typename T, int M>
+__global__ void __launch_bounds__(M / 16)
+phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
+                       const int *__restrict__ nph, const long long *__restrict__ ofs,
+                       const int *__restrict__ stride, const double *__restrict__ phi0,
+                       const double *__restrict__ weight, const int *__restrict__ fftidx,
+                       const FftDesc *__restrict__ fdesc, const double2 *__restrict__ twiddle,
+                       const double2 *__restrict__ wpow2, int P,
+                       const double2 *__restrict__ bhat, const double2 *__restrict__ phase,
+                       int ncm, int mmax, int flags, T *const *__restrict__ maps,
+                       long long map_lo) {
+  constexpr int NT = M / 16;
+  extern __shared__ double2 smem[];
+  double2 *buf = smem;
+  double2 *slo = smem + pw_entries(M);
+  double2 *shi = slo + kShiftLo;
+  const int p = pairs[blockIdx.x >> 1], h = blockIdx.x & 1, c = blockIdx.y;
+  const int ring = 2 * p + h;
+  const int n = nph[ring];
+  if (n <= 0) return;        // unpaired ring: nothing in this hemisphere
+  const int N = n / 2;
+  const FftDesc &fd = fdesc[fftidx[ring]];
+  const double2 *W = twiddle + fd.tw;     // exp(-2 pi i e/n)
+  const double2 *bh = bhat + fd.bhat2;
+  const int ms = mmax + 1;
+  const int mm = min(mmax, mlim[p]);
+  const bool add = (flags & (SHARP_ADD | SHARP_SUBTRACT)) != 0;
+  const double wgt = ((flags & SHARP_USE_WEIGHTS) ? weight[ring] : 1.0) *
+                     ((flags & SHARP_REAL_HARMONICS) ? kSqrtHalf : 1.0) *
+                     ((flags & SHARP_SUBTRACT) ? -1.0 : 1.0);
+  const double ph = phi0[ring];
+  const bool rot = fabs(ph) >= 1e-14;
+  const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
+  if (rot) build_shift(slo, shi, mm, ph);
+  __syncthreads();
+  auto tm = [&](int m) {
+    double2 t = cscale(src[m], wgt);
+    if (rot) t = cmul(t, shift_of(slo, shi, m));
+    return t;
+  };
+  // C_k, k <= N: t_m folded onto bin m mod n, conj t_m onto (n - m) mod n
+  // (sharp.c:265-300); C_0 and C_N real
+  for (int k = threadIdx.x; k <= N; k += NT) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int m = k; m <= mm; m += n) acc = cadd(acc, tm(m));
+    for (int m = (k == 0) ? n : n - k; m <= mm; m += n) acc = cadd(acc, cconj(tm(m)));
+    if (k == 0 || k == N) acc.y = 0.0;
+    buf[pw_pad(k)] = acc;
+  }
+  __syncthreads();
+  // Z_k = (C_k + conj C_{N-k}) + i conj(W^k) (C_k - conj C_{N-k}), k < N,
+  // conjugated and times c_k; zero padding on [N, M/2)
+  auto zin = [&](double2 ck, double2 cn, int k) {
+    cn = cconj(cn);
+    const double2 sm = cadd(ck, cn), df = csub(ck, cn);
+    const double2 w = __ldg(W + k);
+    const double2 iw = make_double2(w.y, w.x);   // i * conj(w)
+    return cmul(cconj(cadd(sm, cmul(iw, df))), pb_chirp(W, k, n));
+  };
+  for (int k = threadIdx.x; 2 * k <= N; k += NT) {
+    const int kk = N - k;
+    const double2 ck = buf[pw_pad(k)], cn = buf[pw_pad(kk)];
+    buf[pw_pad(k)] = zin(ck, cn, k);
+    if (k == 0) buf[pw_pad(N)] = make_double2(0.0, 0.0);
+    else if (kk != k) buf[pw_pad(kk)] = zin(cn, ck, kk);
+  }
+  for (int j = N + 1 + threadIdx.x; j < M / 2; j += NT) buf[pw_pad(j)] = make_double2(0.0, 0.0);
+  __syncthreads();
+  pb_convolve<M>(buf, wpow2, P, bh);
+  // z_j = conj(c_j conv_j): pixels 2j, 2j+1 = Re, Im z_j
+  T *map = maps[c] + (ofs[ring] - map_lo);
+  const long long st = stride[ring];
+  for (int j = threadIdx.x; j < N; j += NT) {
+    const double2 z = cmul(buf[pw_pad(j)], pb_chirp(W, j, n));
+    store_px(map + (2 * j) * st, z.x, add);
+    store_px(map + (2 * j + 1) * st, -z.y, add);
+  }
+}
+
+// ring -> phase
+template <typename T, int M>
+__global__ void __launch_bounds__(M / 16)
+ring2phase_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
+                       const int *__restrict__ nph, const long long *__restrict__ ofs,
+                       const int *__restrict__ stride, const double *__restrict__ phi0,
+                       const double *__restrict__ weight, const int *__restrict__ fftidx,
+                       const FftDesc *__restrict__ fdesc, const double2 *__restrict__ twiddle,
+                       const double2 *__restrict__ wpow2, int P,
+                       const double2 *__restrict__ bhat, double2 *__restrict__ phase, int ncm,
+                       int mmax, int flags, const T *const *__restrict__ maps,
+                       long long map_lo) {
+  constexpr int NT = M / 16;
+  extern __shared__ double2 smem[];
+  double2 *buf = smem;
+  double2 *slo = smem + pw_entries(M);
+  double2 *shi = slo + kShiftLo;
+  const int p = pairs[blockIdx.x >> 1], h = blockIdx.x & 1, c = blockIdx.y;
+  const int ring = 2 * p + h;
+  const int n = nph[ring];
+  if (n <= 0) return;
+  const int N = n / 2;
+  const FftDesc &fd = fdesc[fftidx[ring]];
+  const double2 *W = twiddle + fd.tw;
+  const double2 *bh = bhat + fd.bhat2;
+  const int ms = mmax + 1;
+  const int mm = min(mmax, mlim[p]);
+  const double wgt = ((flags & SHARP_USE_WEIGHTS) ? weight[ring] : 1.0) *
+                     ((flags & SHARP_REAL_HARMONICS) ? kSqrtTwo : 1.0);
+  const double ph = phi0[ring];
+  const bool rot = fabs(ph) >= 1e-14;
+  const T *map = maps[c] + (ofs[ring] - map_lo);
+  const long long st = stride[ring];
+  if (rot) build_shift(slo, shi, mm, -ph);
+  // x_j c_j, x_j = pixels 2j + i (2j+1); zero padding on [N, M/2)
+  for (int j = threadIdx.x; j < M / 2; j += NT) {
+    double2 x = make_double2(0.0, 0.0);
+    if (j < N)
+      x = cmul(make_double2(double(map[(2 * j) * st]), double(map[(2 * j + 1) * st])),
+               pb_chirp(W, j, n));
+    buf[pw_pad(j)] = x;
+  }
+  __syncthreads();
+  pb_convolve<M>(buf, wpow2, P, bh);
+  // Z_k = c_k conv_k (Z_N = Z_0);
+  // X_k = (Z_k + conj Z_{N-k})/2 - i W^k (Z_k - conj Z_{N-k})/2, k <= N
+  auto xout = [&](double2 zk, double2 zn, int k) {
+    zn = cconj(zn);
+    const double2 sm = cadd(zk, zn), df = csub(zk, zn);
+    const double2 w = __ldg(W + k);
+    const double2 mi_w = make_double2(w.y, -w.x);   // -i * w
+    return cscale(cadd(sm, cmul(mi_w, df)), 0.5);
+  };
+  for (int k = threadIdx.x; 2 * k <= N; k += NT) {
+    const int kk = N - k;
+    const double2 zk = cmul(buf[pw_pad(k)], pb_chirp(W, k, n));
+    const double2 zn = (k == 0) ? zk : cmul(buf[pw_pad(kk)], pb_chirp(W, kk, n));
+    double2 xk = xout(zk, zn, k), xn = xout(zn, zk, kk);
+    if (k == 0) { xk.y = 0.0; xn.y = 0.0; }   // DC and Nyquist are real
+    buf[pw_pad(k)] = xk;
+    if (kk != k) buf[pw_pad(kk)] = xn;
+  }
+  __syncthreads();
+  // phase_m = X_{m mod n} (conjugated above N) wgt e^{-i m phi0}, m <= mm
+  double2 *dst = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
+  for (int m = threadIdx.x; m <= mm; m += NT) {
+    const int idx = m % n;
+    double2 v = (idx <= N) ? buf[pw_pad(idx)] : cconj(buf[pw_pad(n - idx)]);
+    v = cscale(v, wgt);
+    if (rot) v = cmul(v, shift_of(slo, shi, m));
+    dst[m] = v;
   }
 }
 
@@ -1128,10 +1419,31 @@ void launch_twiddles(GeomPlan &gp, int ntw, const std::vector<int> &tw_n,
 // Ring pairs are launched per size class (largest complex FFT length of
 // the pair <= cls_N[c]) so small polar rings do not reserve the shared
 // memory and threads of the largest rings.
-void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cudaStream_t st) {
-  std::vector<int> idx;
-  for (int i = 0; i < int(descs.size()); ++i)
-    if (descs[i].blue) idx.push_back(i);
+namespace {
+
+// The register-pass chirp spectra, one launch per convolution length.
+void launch_bluestein_pw_setup(const GeomPlan &gp, const int *d_blue2_idx, int nblue2,
+                               cudaStream_t st) {
+  if (nblue2 <= 0) return;
+  ProfScope ps("bluestein_setup", st);
+  auto one = [&](auto kernel, int M) {
+    const size_t smem = sizeof(double2) * pw_entries(M);
+    SHT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem)));
+    kernel<<<nblue2, M / 16, smem, st>>>(gp.fdesc, d_blue2_idx, gp.twiddle, gp.wpow2, gp.P,
+                                         gp.bhat);
+    SHT_CUDA(cudaGetLastError());
+  };
+  if (gp.P >= 1024) one(bluestein_pw_setup_kernel<1024>, 1024);
+  if (gp.P >= 2048) one(bluestein_pw_setup_kernel<2048>, 2048);
+  if (gp.P >= 4096) one(bluestein_pw_setup_kernel<4096>, 4096);
+  if (gp.P >= 8192) one(bluestein_pw_setup_kernel<8192>, 8192);
+}
+
+}  // namespace
+
+void launch_bluestein_setup(GeomPlan &gp, const GeomHost &h, cudaStream_t st) {
+  const std::vector<int> &idx = h.blue_idx;
   // exp(-2 pi i j/P) for the power-of-two passes (computed even when unused)
   std::vector<int> pn{gp.P}, po{0};
   {
@@ -1146,15 +1458,26 @@ void launch_bluestein_setup(GeomPlan &gp, const std::vector<FftDesc> &descs, cud
     SHT_CUDA(cudaFreeAsync(d_n, st));
     SHT_CUDA(cudaFreeAsync(d_off, st));
   }
-  if (idx.empty()) return;
-  int *d_idx = nullptr;
-  SHT_CUDA(::sht::ws_alloc(&d_idx, sizeof(int) * idx.size(), st));
-  SHT_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st));
-  ProfScope ps("bluestein_setup", st);
-  bluestein_setup_kernel<<<int(idx.size()), 256, 0, st>>>(gp.fdesc, d_idx, gp.twiddle, gp.wpow2,
-                                                          gp.P, gp.bhat);
-  SHT_CUDA(cudaGetLastError());
-  SHT_CUDA(cudaFreeAsync(d_idx, st));
+  if (!idx.empty()) {
+    int *d_idx = nullptr;
+    SHT_CUDA(::sht::ws_alloc(&d_idx, sizeof(int) * idx.size(), st));
+    SHT_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(),
+                             cudaMemcpyHostToDevice, st));
+    ProfScope ps("bluestein_setup", st);
+    bluestein_setup_kernel<<<int(idx.size()), 256, 0, st>>>(gp.fdesc, d_idx, gp.twiddle,
+                                                            gp.wpow2, gp.P, gp.bhat);
+    SHT_CUDA(cudaGetLastError());
+    SHT_CUDA(cudaFreeAsync(d_idx, st));
+  }
+  const std::vector<int> &idx2 = h.blue2_idx;
+  if (!idx2.empty()) {
+    int *d_idx = nullptr;
+    SHT_CUDA(::sht::ws_alloc(&d_idx, sizeof(int) * idx2.size(), st));
+    SHT_CUDA(cudaMemcpyAsync(d_idx, idx2.data(), sizeof(int) * idx2.size(),
+                             cudaMemcpyHostToDevice, st));
+    launch_bluestein_pw_setup(gp, d_idx, int(idx2.size()), st);
+    SHT_CUDA(cudaFreeAsync(d_idx, st));
+  }
 }
 
 static size_t fft_smem(const GeomPlan &gp, int cls, int mmax) {
@@ -1268,6 +1591,34 @@ void ring2phase_pow2(const JobDesc &job, const GeomPlan &gp, int cls, long long 
   SHT_CUDA(cudaGetLastError());
 }
 
+template <typename T, int M>
+void phase2ring_blue(const JobDesc &job, const GeomPlan &gp, int cls, long long map_lo,
+                     const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
+                     cudaStream_t st) {
+  auto k = phase2ring_blue_kernel<T, M>;
+  const size_t smem = pow2_smem(M, job.mmax);
+  SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  k<<<dim3(2 * gp.pb_count[cls], nmapptr), M / 16, smem, st>>>(
+      gp.pb_pairs + gp.pb_start[cls], gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
+      gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm, job.mmax, job.flags,
+      reinterpret_cast<T *const *>(maps_dev), map_lo);
+  SHT_CUDA(cudaGetLastError());
+}
+
+template <typename T, int M>
+void ring2phase_blue(const JobDesc &job, const GeomPlan &gp, int cls, long long map_lo,
+                     const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
+                     cudaStream_t st) {
+  auto k = ring2phase_blue_kernel<T, M>;
+  const size_t smem = pow2_smem(M, job.mmax);
+  SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  k<<<dim3(2 * gp.pb_count[cls], nmapptr), M / 16, smem, st>>>(
+      gp.pb_pairs + gp.pb_start[cls], gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
+      gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm, job.mmax, job.flags,
+      reinterpret_cast<const T *const *>(maps_dev), map_lo);
+  SHT_CUDA(cudaGetLastError());
+}
+
 template <typename T>
 void phase2ring_pow2_classes(const JobDesc &job, const GeomPlan &gp, long long map_lo,
                              const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
@@ -1279,6 +1630,15 @@ void phase2ring_pow2_classes(const JobDesc &job, const GeomPlan &gp, long long m
       case 2048: phase2ring_pow2<T, 2048>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
       case 4096: phase2ring_pow2<T, 4096>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
       default: phase2ring_pow2<T, 8192>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+    }
+  }
+  for (int c = 0; c < int(gp.pb_M.size()); ++c) {
+    if (gp.pb_count[c] == 0) continue;
+    switch (gp.pb_M[c]) {
+      case 1024: phase2ring_blue<T, 1024>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+      case 2048: phase2ring_blue<T, 2048>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+      case 4096: phase2ring_blue<T, 4096>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
+      default: phase2ring_blue<T, 8192>(job, gp, c, map_lo, phase, ncm, maps_dev, nmapptr, st); break;
     }
   }
 }
@@ -1294,6 +1654,15 @@ void ring2phase_pow2_classes(const JobDesc &job, const GeomPlan &gp, long long m
       case 2048: ring2phase_pow2<T, 2048>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
       case 4096: ring2phase_pow2<T, 4096>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
       default: ring2phase_pow2<T, 8192>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+    }
+  }
+  for (int c = 0; c < int(gp.pb_M.size()); ++c) {
+    if (gp.pb_count[c] == 0) continue;
+    switch (gp.pb_M[c]) {
+      case 1024: ring2phase_blue<T, 1024>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+      case 2048: ring2phase_blue<T, 2048>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+      case 4096: ring2phase_blue<T, 4096>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
+      default: ring2phase_blue<T, 8192>(job, gp, c, map_lo, maps_dev, nmapptr, phase, ncm, st); break;
     }
   }
 }
@@ -1419,12 +1788,14 @@ void launch_twiddles_preplaced(double2 *tw, const int *d_n, const int *d_off, in
 }
 
 void launch_bluestein_setup_preplaced(const GeomPlan &gp, const int *d_blue_idx, int nblue,
-                                      cudaStream_t st) {
-  if (nblue <= 0) return;
-  ProfScope ps("bluestein_setup", st);
-  bluestein_setup_kernel<<<nblue, 256, 0, st>>>(gp.fdesc, d_blue_idx, gp.twiddle, gp.wpow2,
-                                                gp.P, gp.bhat);
-  SHT_CUDA(cudaGetLastError());
+                                      const int *d_blue2_idx, int nblue2, cudaStream_t st) {
+  if (nblue > 0) {
+    ProfScope ps("bluestein_setup", st);
+    bluestein_setup_kernel<<<nblue, 256, 0, st>>>(gp.fdesc, d_blue_idx, gp.twiddle, gp.wpow2,
+                                                  gp.P, gp.bhat);
+    SHT_CUDA(cudaGetLastError());
+  }
+  launch_bluestein_pw_setup(gp, d_blue2_idx, nblue2, st);
 }
 
 }  // namespace sht

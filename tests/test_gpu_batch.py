@@ -198,3 +198,51 @@ def test_config2_full_size_per_map_errors():
         ref.execute(sb.SHARP_MAP2ALM, spin, back, [x.copy() for x in m64[i]], g, a, 1, DP)
         for x, y in zip(a64[i], back):
             assert rel_l2(x, y) < 1e-12
+
+
+def test_config2_device_batch_runs_groups_side_by_side():
+    # the batched configuration with device arrays: one batch call runs its
+    # six merged groups (spin x Nside) side by side on library streams; the
+    # outputs equal those of the same groups run one after another, bit for
+    # bit, and the two times are printed
+    import torch
+    geo, sets = _mix(nsides=(256, 512, 1024), n0=48, n2=16, seed=6)
+    dev = torch.device("cuda:0")
+
+    def dalm(x):
+        return torch.view_as_real(torch.from_numpy(x).to(dev)).reshape(-1)
+
+    alms = [[dalm(x) for x in s[2]] for s in sets]
+    out_b = [[torch.zeros(12 * s[1] ** 2, dtype=torch.float64, device=dev) for _ in s[2]]
+             for s in sets]
+    out_s = [[torch.zeros_like(x) for x in o] for o in out_b]
+    for flags in (DP, DP | MIXED):
+        jobs_b = [(sb.SHARP_ALM2MAP, s[0], a, o, *geo[s[1]], 1, flags)
+                  for s, a, o in zip(sets, alms, out_b)]
+        sb.execute_batch(jobs_b, device=True)          # warm-up: plans, tables
+        # the same merged groups, one after another on the current stream
+        groups = {}
+        for s, a, o in zip(sets, alms, out_s):
+            g = groups.setdefault((s[0], s[1]), ([], []))
+            g[0].extend(a)
+            g[1].extend(o)
+        def sequential():
+            for (spin, n), (a, o) in groups.items():
+                nt = len(a) // (1 if spin == 0 else 2)
+                sb.execute_device(sb.SHARP_ALM2MAP, spin, a, o, *geo[n], nt, flags)
+        sequential()
+        torch.cuda.synchronize()
+        times = {}
+        for name, fn in (("batch", lambda: sb.execute_batch(jobs_b, device=True)),
+                         ("sequential", sequential)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            times[name] = e0.elapsed_time(e1)
+        print(f"config 2 alm2map, {'mixed' if flags & MIXED else 'FP64'}: batch "
+              f"{times['batch']:.1f} ms, groups one after another {times['sequential']:.1f} ms")
+        for xb, xs in zip(out_b, out_s):
+            for x, y in zip(xb, xs):
+                assert torch.equal(x, y)

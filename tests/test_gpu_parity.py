@@ -506,3 +506,62 @@ def test_prime_ring_lengths_match_reference(ref, spin):
     ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, DP)
     for x, y in zip(b1, b2):
         assert rel_l2(x, y) < TOL
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+@pytest.mark.parametrize("flags", [DP, 0])
+def test_register_bluestein_rings_match_reference(ref, spin, flags):
+    # even rings whose half length has a large prime factor: Bluestein
+    # convolution lengths 1024 (1018 = 2 * 509), 2048 (2004 = 4 * 3 * 167),
+    # 4096 (2062 = 2 * 1031) and 8192 (4124 = 4 * 1031, the polar HEALPix
+    # form 4i); alias folding (lmax above half the shorter rings), phi0
+    # shifts, weights, an interleaved stride-2 pair, an unpaired ring and a
+    # pair of unequal lengths (which takes the size-class kernels); both
+    # directions, FP64 and single-precision I/O
+    rings = [  # (nph, theta, phi0, stride)
+        (1018, 0.7, 0.1, 1), (1018, np.pi - 0.7, 0.1, 1),
+        (2004, 0.9, 0.0, 1), (2004, np.pi - 0.9, 0.0, 1),
+        (2062, 1.1, 0.3, 1), (2062, np.pi - 1.1, 0.3, 1),
+        (4124, 1.3, 0.05, 1), (4124, np.pi - 1.3, 0.05, 1),
+        (1018, 1.45, 0.2, 2), (1018, np.pi - 1.45, 0.2, 2),
+        (2004, np.pi / 2, 0.4, 1),
+        (1018, 0.5, 0.0, 1), (2004, np.pi - 0.5, 0.0, 1),
+    ]
+    nph = np.array([r[0] for r in rings], np.int32)
+    theta = np.array([r[1] for r in rings])
+    phi0 = np.array([r[2] for r in rings])
+    st = np.array([r[3] for r in rings], np.int32)
+    ofs = np.zeros(len(rings), np.intp)
+    pos = 0
+    for i, r in enumerate(rings):
+        if r[3] == 2 and i > 0 and rings[i - 1][3] == 2:
+            ofs[i] = ofs[i - 1] + 1         # interleaved with the previous ring
+            pos = ofs[i - 1] + 2 * r[0]
+        else:
+            ofs[i] = pos
+            pos += r[0] * r[3]
+    npix = int(pos)
+    w = np.linspace(0.5, 1.5, len(rings)) * 4 * np.pi / npix
+    g1 = sb.Geometry.general(nph, ofs, st, phi0, theta, w)
+    g2 = ref.general(nph, ofs, st, phi0, theta, w)
+    lmax = 1100
+    a1, a2 = sb.AlmInfo.triangular(lmax), ref.triangular(lmax, lmax)
+    nreal = np.float64 if flags & DP else np.float32
+    ncpx = np.complex128 if flags & DP else np.complex64
+    tol = TOL if flags & DP else 1e-6
+    na = _nalm(1, spin)
+    alms = [uniform_alm(lmax, seed=90 + i, spin=spin).astype(ncpx) for i in range(na)]
+    m1 = [np.zeros(npix, nreal) for _ in range(na)]
+    m2 = [np.zeros(npix, nreal) for _ in range(na)]
+    sb.execute(1, spin, [x.copy() for x in alms], m1, g1, a1, 1, flags)
+    ref.execute(1, spin, [x.copy() for x in alms], m2, g2, a2, 1, flags)
+    for x, y in zip(m1, m2):
+        assert rel_l2(x, y) < tol
+    rng = np.random.default_rng(23 + spin)
+    maps = [rng.standard_normal(npix).astype(nreal) for _ in range(na)]
+    b1 = [np.zeros(sb.nalm_triangular(lmax), ncpx) for _ in range(na)]
+    b2 = [x.copy() for x in b1]
+    sb.execute(0, spin, b1, [x.copy() for x in maps], g1, a1, 1, flags)
+    ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, flags)
+    for x, y in zip(b1, b2):
+        assert rel_l2(x, y) < tol
