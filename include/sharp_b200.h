@@ -116,23 +116,28 @@ typedef struct {
   int flags;
 } sharp_b200_job;
 
-/* Runs a batch of independent jobs of uneven geometry, lmax and spin (for
-   example many spin-0 and spin-2 maps at several HEALPix resolutions).
-   No counterpart in the reference, whose callers loop over sharp_execute.
-   Jobs that share type, spin, flags and the same geom_info and alm_info
-   objects are merged into one job of up to 100 transforms, so the batched
-   kernels (SHARP_MIXED) see them together.  Every output equals that of
-   sharp_execute on its own job (neither the merge nor the scheduling
-   changes any arithmetic).  Jobs must not share output arrays.
-   device_ptrs = 0: host arrays; all merged jobs run as one pipelined
-   sequence of pieces (host->device copies, compute and device->host copies
-   overlapped across the whole batch); returns after the results are copied
-   back.  device_ptrs = 1: device arrays; the merged jobs run side by side on
-   up to four library streams forked from `stream` and joined back to it
-   (work ordered after what `stream` holds, later work on `stream` after the
-   batch), without host synchronisation.  opcnt (if non-NULL) receives the
-   summed operation count.  Returns the number of merged groups executed,
-   or -1 after a failure in non-abort mode. */
+/* Runs a batch of jobs of uneven geometry, lmax and spin (for example many
+   spin-0 and spin-2 maps at several HEALPix resolutions, or the alm2map and
+   map2alm halves of a round trip).  No counterpart in the reference, whose
+   callers loop over sharp_execute.  Jobs that share type, spin, flags and
+   the same geom_info and alm_info objects are merged into one job of up to
+   100 transforms, so the batched kernels (SHARP_MIXED) see them together.
+   Every output equals that of sharp_execute on its own job, run in list
+   order (neither the merge nor the scheduling changes any arithmetic).
+   Jobs must not share output arrays.
+   device_ptrs = 0: host arrays; the jobs take effect in list order: a job
+   may read host arrays that an earlier job of the batch writes (its input
+   copies wait for those output copies; in such a batch only consecutive
+   jobs are merged).  All merged jobs run as one pipelined sequence of pieces
+   (host->device copies, compute and device->host copies overlapped across
+   the whole batch); returns after the results are copied back.
+   device_ptrs = 1: device arrays; the jobs must be independent (no job reads
+   another's output), any compatible jobs are merged, and the merged jobs
+   run side by side on up to four library streams forked from `stream` and
+   joined back to it (work ordered after what `stream` holds, later work on
+   `stream` after the batch), without host synchronisation.  opcnt (if
+   non-NULL) receives the summed operation count.  Returns the number of
+   merged groups executed, or -1 after a failure in non-abort mode. */
 int sharp_b200_execute_batch (const sharp_b200_job *jobs, int njobs,
   int device_ptrs, void *stream, unsigned long long *opcnt);
 

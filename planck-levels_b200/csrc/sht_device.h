@@ -30,8 +30,8 @@ struct FftDesc {
   int tw;       // offset of exp(-2 pi i j/n), j<n, in the twiddle table
   int nrad;
   int rad[kMaxRadices];
-  int blue;     // 1: Bluestein convolution of power-of-two length M
-  int M;
+  int blue;     // 1: the size-class kernels run a Bluestein convolution of length M
+  int M;       // power-of-two convolution length >= 2N - 1
   long long bhat;   // offset of the transformed chirp in the digit order of the
                     // radix-4 stages (/M), or -1 when no generic-class ring uses it
   long long bhat2;  // the same in the digit order of the radix-16 register passes,
@@ -82,11 +82,16 @@ inline int pow2_ring_length(int nph, int stride, int mm) {
   if (N != 1024 && N != 2048 && N != 4096 && N != 8192) return 0;
   return mm <= N ? N : 0;
 }
-// Convolution length M of a ring that the register Bluestein kernels take
-// (even nph whose complex length uses the Bluestein convolution with M in
-// {1024, 2048, 4096, 8192}; any stride, any alias folding), else 0.
+// Convolution length M of a ring that the register Bluestein kernels take,
+// else 0: even nph with M in {1024, 2048, 4096, 8192} (any stride, any alias
+// folding) whose complex length either calls for a Bluestein convolution by
+// the cost model of the size classes or exceeds 1024 (there the size-class
+// kernel, one 1024-thread CTA per SM, ran the mixed-radix Stockham passes
+// about twice as slowly per ring as the register convolution).
+constexpr int kRegBluesteinMinN = 1024;
 inline int blue_ring_length(int nph, const FftDesc &d) {
-  if (nph <= 0 || (nph & 1) || !d.blue) return 0;
+  if (nph <= 0 || (nph & 1)) return 0;
+  if (!d.blue && d.N <= kRegBluesteinMinN) return 0;
   return (d.M == 1024 || d.M == 2048 || d.M == 4096 || d.M == 8192) ? d.M : 0;
 }
 GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin);

@@ -233,7 +233,7 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
         while (M < 2 * d.N - 1) { M <<= 1; ++lg; }
         const long long blue_cost = 2ll * ((long long)M * lg + 2ll * d.N);
         d.blue = (d.N > 16 && blue_cost < direct) ? 1 : 0;
-        d.M = d.blue ? M : 0;
+        d.M = M;   // the convolution length, also for rings the register Bluestein takes
         d.bhat = d.bhat2 = -1;
         h.tw_n.push_back(d.n);
         h.tw_off.push_back(int(h.tw_total));
@@ -253,8 +253,6 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
     }
   }
   SHT_REQUIRE(h.tw_total < (1ll << 31), "geometry too large (twiddle table)");
-  for (const FftDesc &d : h.descs)
-    if (d.blue) h.P = std::max(h.P, d.M);
   // rings tile [lo,hi) exactly -> synthesis need not pre-load the map
   bool covered = unit_stride && !spans.empty();
   if (covered) {
@@ -275,7 +273,7 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
   // length); a length whose buffer and phi0 slices exceed the shared memory
   // of a CTA stays in the size classes
   std::map<int, std::vector<int>> pw_lists, pb_lists;
-  std::vector<char> is_pw(np, 0);
+  std::vector<char> is_pw(np, 0);   // 1: power-of-two pair, 2: register Bluestein pair
   auto fits = [&](int len) {
     return sizeof(double2) * pow2_ring_smem_entries(len, mmax) <= kRingSmemLimit;
   };
@@ -295,7 +293,7 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
       is_pw[p] = 1;
     } else if (M > 0 && fits(M)) {
       pb_lists[M].push_back(p);
-      is_pw[p] = 1;
+      is_pw[p] = 2;
     }
   }
   for (auto &kv : pw_lists) {
@@ -350,8 +348,10 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
   for (int p = 0; p < np; ++p)
     for (int hh = 0; hh < 2; ++hh) {
       const int i = 2 * p + hh;
-      if (h.nph[i] <= 0 || !h.descs[h.fft[i]].blue) continue;
-      (is_pw[p] ? use16 : use4)[h.fft[i]] = 1;
+      if (h.nph[i] <= 0) continue;
+      const FftDesc &d = h.descs[h.fft[i]];
+      if (is_pw[p] == 0 && d.blue) use4[h.fft[i]] = 1;
+      if (is_pw[p] == 2) use16[h.fft[i]] = 1;   // register Bluestein pairs
     }
   for (int i = 0; i < int(h.descs.size()); ++i) {
     FftDesc &d = h.descs[i];
@@ -365,6 +365,7 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
       h.bhat_total += d.M;
       h.blue2_idx.push_back(i);
     }
+    if (use4[i] || use16[i]) h.P = std::max(h.P, d.M);
   }
   return h;
 }
@@ -909,23 +910,45 @@ struct HostJob {
 // Runs host-array jobs as one sequence of pieces (see above): the copies of
 // consecutive pieces overlap the compute across job boundaries too, so a
 // list of jobs has one fill and one drain.  Every job must satisfy
-// pipelinable(); the jobs must be independent (no job reads another's
-// output).  *opcnt receives the summed operation count of the jobs.
+// pipelinable().  A job may read host arrays that an earlier job of the
+// list writes (a round trip: alm2map, then map2alm of its maps): the input
+// copy of such bytes waits for the output copy of the piece that wrote
+// them, so the data passes through host memory in order while the other
+// pieces keep the copy engines and the GPU busy.  (Writes after reads and
+// after writes are ordered already: every output copy follows the compute
+// of its piece, which follows all earlier input copies, on one output
+// stream.)  *opcnt receives the summed operation count of the jobs.
 void execute_pipelined_jobs(const std::vector<HostJob> &jobs, unsigned long long *opcnt) {
   cudaStream_t cs = library_stream();
   cudaStream_t sin = copy_stream(0), sout = copy_stream(1);
   // window buffers of one piece, released on the output stream after its copies
   struct Piece {
     std::vector<void *> dmap, dalm;
-    cudaEvent_t in_done = nullptr, compute_done = nullptr;
+    cudaEvent_t in_done = nullptr, compute_done = nullptr, out_done = nullptr;
   };
   std::vector<Piece> pieces;
+  // host byte ranges written by the output copies so far: [lo, hi), piece
+  struct Written {
+    uintptr_t lo, hi;
+    int piece;
+  };
+  std::vector<Written> written;
+  // makes the input stream wait for the last output copy that wrote any of
+  // [src, src + bytes)
+  auto order_after_writes = [&](const void *src, size_t bytes) {
+    const uintptr_t lo = reinterpret_cast<uintptr_t>(src), hi = lo + bytes;
+    int last = -1;
+    for (const Written &w : written)
+      if (w.lo < hi && lo < w.hi) last = std::max(last, w.piece);
+    if (last >= 0) SHT_CUDA(cudaStreamWaitEvent(sin, pieces[last].out_done, 0));
+  };
   auto release = [&]() {
     for (auto &pc : pieces) {
       for (void *p : pc.dmap) if (p) cudaFreeAsync(p, sout);
       for (void *p : pc.dalm) if (p) cudaFreeAsync(p, sout);
       if (pc.in_done) cudaEventDestroy(pc.in_done);
       if (pc.compute_done) cudaEventDestroy(pc.compute_done);
+      if (pc.out_done) cudaEventDestroy(pc.out_done);
     }
     pieces.clear();
   };
@@ -968,17 +991,25 @@ void execute_pipelined_jobs(const std::vector<HostJob> &jobs, unsigned long long
         pc.dalm.assign(size_t(nt) * ncomp, nullptr);
         SHT_CUDA(cudaEventCreateWithFlags(&pc.in_done, cudaEventDisableTiming));
         SHT_CUDA(cudaEventCreateWithFlags(&pc.compute_done, cudaEventDisableTiming));
+        SHT_CUDA(cudaEventCreateWithFlags(&pc.out_done, cudaEventDisableTiming));
+        const int this_piece = int(pieces.size()) - 1;
         // inputs of the piece: host -> device on the input stream
         for (int i = 0; i < nt * ncomp; ++i) {
           const int gi = t0p * ncomp + i;
           SHT_CUDA(::sht::ws_alloc(&pc.dmap[i], esz_map * std::max<long long>(map_n, 1), sin));
           SHT_CUDA(::sht::ws_alloc(&pc.dalm[i], esz_alm * std::max<long long>(alm_n, 1), sin));
-          if (load_maps && map_n > 0)
-            SHT_CUDA(cudaMemcpyAsync(pc.dmap[i], static_cast<char *>(map_in[gi]) + esz_map * map_lo,
-                                     esz_map * map_n, cudaMemcpyHostToDevice, sin));
-          if (load_alm && alm_n > 0)
-            SHT_CUDA(cudaMemcpyAsync(pc.dalm[i], static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
-                                     esz_alm * alm_n, cudaMemcpyHostToDevice, sin));
+          if (load_maps && map_n > 0) {
+            const char *src = static_cast<char *>(map_in[gi]) + esz_map * map_lo;
+            order_after_writes(src, esz_map * map_n);
+            SHT_CUDA(cudaMemcpyAsync(pc.dmap[i], src, esz_map * map_n, cudaMemcpyHostToDevice,
+                                     sin));
+          }
+          if (load_alm && alm_n > 0) {
+            const char *src = static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo;
+            order_after_writes(src, esz_alm * alm_n);
+            SHT_CUDA(cudaMemcpyAsync(pc.dalm[i], src, esz_alm * alm_n, cudaMemcpyHostToDevice,
+                                     sin));
+          }
         }
         SHT_CUDA(cudaEventRecord(pc.in_done, sin));
         // compute on the library stream: a device-pointer job whose array
@@ -998,15 +1029,24 @@ void execute_pipelined_jobs(const std::vector<HostJob> &jobs, unsigned long long
         SHT_CUDA(cudaStreamWaitEvent(sout, pc.compute_done, 0));
         for (int i = 0; i < nt * ncomp; ++i) {
           const int gi = t0p * ncomp + i;
+          char *dst = nullptr;
+          size_t bytes = 0;
           if (analysis) {
-            if (alm_n > 0)
-              SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo,
-                                       pc.dalm[i], esz_alm * alm_n, cudaMemcpyDeviceToHost, sout));
+            if (alm_n > 0) {
+              dst = static_cast<char *>(alm_in[gi]) + esz_alm * alm_lo;
+              bytes = esz_alm * alm_n;
+              SHT_CUDA(cudaMemcpyAsync(dst, pc.dalm[i], bytes, cudaMemcpyDeviceToHost, sout));
+            }
           } else if (map_n > 0) {
-            SHT_CUDA(cudaMemcpyAsync(static_cast<char *>(map_in[gi]) + esz_map * map_lo,
-                                     pc.dmap[i], esz_map * map_n, cudaMemcpyDeviceToHost, sout));
+            dst = static_cast<char *>(map_in[gi]) + esz_map * map_lo;
+            bytes = esz_map * map_n;
+            SHT_CUDA(cudaMemcpyAsync(dst, pc.dmap[i], bytes, cudaMemcpyDeviceToHost, sout));
           }
+          if (bytes)
+            written.push_back(Written{reinterpret_cast<uintptr_t>(dst),
+                                      reinterpret_cast<uintptr_t>(dst) + bytes, this_piece});
         }
+        SHT_CUDA(cudaEventRecord(pc.out_done, sout));
       }
       // the count of one call with all transforms (per-triple weight of
       // sharp_core_inc2.c:173,442): the pieces share the triples
@@ -1052,10 +1092,49 @@ bool guarded(const std::function<void()> &fn) {
   }
 }
 
-// Batch of independent jobs: jobs with the same type, spin, flags, geometry
-// and a_lm objects are merged (their pointer arrays concatenated in order) into
-// jobs of at most kMaxTrans transforms; each merged job runs through
-// execute_impl.  Returns the number of merged jobs.
+// Host byte range [lo, hi) that one array of a job spans (maps: the ring
+// pixels; a_lm: the layout's entries), from the geometry and a_lm structs.
+std::pair<uintptr_t, uintptr_t> host_span(const void *base, const sharp_b200_job &j, bool maps) {
+  const size_t ereal = (j.flags & SHARP_DP) ? 8 : 4;
+  long long lo = 0, hi = 0;
+  bool first = true;
+  auto take = [&](long long a, long long b) {
+    const long long mn = std::min(a, b), mx = std::max(a, b) + 1;
+    if (first) { lo = mn; hi = mx; first = false; }
+    lo = std::min(lo, mn);
+    hi = std::max(hi, mx);
+  };
+  size_t esz = ereal;
+  if (maps) {
+    const sharp_geom_info *g = j.geom_info;
+    for (int p = 0; p < g->npairs; ++p)
+      for (int h = 0; h < 2; ++h) {
+        const sharp_ringinfo &r = h ? g->pair[p].r2 : g->pair[p].r1;
+        if (r.nph > 0) take(r.ofs, r.ofs + (long long)(r.nph - 1) * r.stride);
+      }
+  } else {
+    const sharp_alm_info *a = j.alm_info;
+    const bool packed = (a->flags & SHARP_PACKED) != 0;
+    esz = packed ? ereal : 2 * ereal;
+    for (int mi = 0; mi < a->nm; ++mi) {
+      const int m = a->mval[mi];
+      if (m > a->lmax) continue;
+      const long long s = a->stride, e = packed && m != 0 ? 2 : 1;
+      const long long i0 = a->mvstart[mi] + e * m * s, i1 = a->mvstart[mi] + e * a->lmax * s;
+      take(i0, i1);
+      take(i0 + e - 1, i1 + e - 1);   // the imaginary entries of a packed layout
+    }
+  }
+  const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+  return {b + uintptr_t(lo * (long long)esz), b + uintptr_t(hi * (long long)esz)};
+}
+
+// Batch of jobs: jobs with the same type, spin, flags, geometry and a_lm
+// objects are merged (their pointer arrays concatenated in order) into jobs
+// of at most kMaxTrans transforms; each merged job runs through
+// execute_impl.  With host arrays a job may read what an earlier job writes:
+// such batches merge only consecutive jobs, so that no job moves ahead of
+// one it depends on.  Returns the number of merged jobs.
 int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
                        cudaStream_t stream, unsigned long long *opcnt) {
   SHT_REQUIRE(njobs >= 0 && (jobs != nullptr || njobs == 0), "bad job list");
@@ -1075,10 +1154,54 @@ int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
     const sharp_b200_job &j = jobs[i];
     SHT_REQUIRE(j.ntrans > 0 && j.ntrans <= kMaxTrans, "bad number of simultaneous transforms");
     SHT_REQUIRE(j.alm != nullptr && j.map != nullptr, "null alm or map pointer array");
+    SHT_REQUIRE(j.geom_info != nullptr && j.alm_info != nullptr, "null geometry or a_lm info");
+  }
+  // host arrays: does any job read bytes that another job writes?
+  bool dependent = false;
+  if (!device_ptrs) {
+    struct Span {
+      uintptr_t lo, hi;
+      int job;
+    };
+    std::vector<Span> reads, writes;
+    for (int i = 0; i < njobs; ++i) {
+      const sharp_b200_job &j = jobs[i];
+      int na, nm;
+      counts(j, na, nm);
+      const bool to_alm = j.type == SHARP_MAP2ALM || j.type == SHARP_Yt;
+      void *const *pa = static_cast<void *const *>(j.alm);
+      void *const *pm = static_cast<void *const *>(j.map);
+      for (int t = 0; t < j.ntrans * na; ++t) {
+        if (!pa[t]) continue;
+        const auto sp = host_span(pa[t], j, false);
+        (to_alm ? writes : reads).push_back(Span{sp.first, sp.second, i});
+      }
+      for (int t = 0; t < j.ntrans * nm; ++t) {
+        if (!pm[t]) continue;
+        const auto sp = host_span(pm[t], j, true);
+        (to_alm ? reads : writes).push_back(Span{sp.first, sp.second, i});
+      }
+    }
+    for (const Span &r : reads) {
+      for (const Span &w : writes)
+        if (r.job != w.job && r.lo < w.hi && w.lo < r.hi) {
+          dependent = true;
+          break;
+        }
+      if (dependent) break;
+    }
+  }
+  for (int i = 0; i < njobs; ++i) {
+    const sharp_b200_job &j = jobs[i];
     int na, nm;
     counts(j, na, nm);
+    // independent jobs: any earlier group; a host batch with dependences:
+    // the last group only, so that merging never moves a job ahead of one
+    // it depends on
     Group *g = nullptr;
-    for (auto &c : groups) {
+    for (size_t k = dependent ? (groups.empty() ? 0 : groups.size() - 1) : 0;
+         k < groups.size(); ++k) {
+      Group &c = groups[k];
       const sharp_b200_job &f = *c.first;
       if (f.type == j.type && f.spin == j.spin && f.flags == j.flags &&
           f.geom_info == j.geom_info && f.alm_info == j.alm_info &&

@@ -345,7 +345,11 @@ def execute_batch(jobs, device: bool = False, stream=None):
     (jtype, spin, alm, maps, geom, ainfo, ntrans, flags) with alm/maps lists
     of numpy arrays (device=False) or CUDA tensors (device=True), as in
     ``execute`` / ``execute_device``.  Compatible jobs are merged into one
-    batched job.  Returns (number of merged jobs, operation count)."""
+    batched job.  With host arrays the jobs take effect in list order (a
+    job may read arrays an earlier job writes, e.g. the alm2map and map2alm
+    halves of a round trip; only consecutive jobs merge); with device arrays
+    the jobs must be independent.  Returns (number of merged jobs, operation
+    count)."""
     keep = []
     arr = (sharp_b200_job * max(len(jobs), 1))()
     for i, (jt, spin, alm, maps, geom, ainfo, nt, fl) in enumerate(jobs):

@@ -246,3 +246,51 @@ def test_config2_device_batch_runs_groups_side_by_side():
         for xb, xs in zip(out_b, out_s):
             for x, y in zip(xb, xs):
                 assert torch.equal(x, y)
+
+
+def test_host_batch_round_trip_in_one_call():
+    # alm2map jobs and the map2alm jobs of their maps in one host-array call:
+    # the map2alm input copies must wait for the alm2map output copies (the
+    # maps start as zeros).  The maps are slices of one buffer (each its own
+    # base pointer), several pieces per job, spin 0 and 2; a third job
+    # compatible with the first comes after the dependent ones and must not
+    # be merged ahead of them.  Every output equals the sequential calls.
+    nside, lmax, nt = 32, 64, 7
+    g, a = sb.Geometry.healpix(nside), sb.AlmInfo.triangular(lmax)
+    npix, nalm = 12 * nside * nside, sb.nalm_triangular(lmax)
+    rng = np.random.default_rng(11)
+    cl = _cl(lmax)
+    alm0 = [_alm(lmax, cl, rng) for _ in range(nt)]
+    alm2 = [_alm(lmax, 0.1 * cl, rng) for _ in range(2 * nt)]
+    big = np.zeros(3 * nt * npix)
+    m0 = [big[i * npix:(i + 1) * npix] for i in range(nt)]
+    m2 = [big[(nt + i) * npix:(nt + i + 1) * npix] for i in range(2 * nt)]
+    o0 = [np.zeros(nalm, np.complex128) for _ in range(nt)]
+    o2 = [np.zeros(nalm, np.complex128) for _ in range(2 * nt)]
+    extra = [np.zeros(npix) for _ in range(2)]
+    jobs = [(sb.SHARP_ALM2MAP, 0, alm0, m0, g, a, nt, DP),
+            (sb.SHARP_ALM2MAP, 2, alm2, m2, g, a, nt, DP),
+            (sb.SHARP_MAP2ALM, 0, o0, m0, g, a, nt, DP),
+            (sb.SHARP_MAP2ALM, 2, o2, m2, g, a, nt, DP),
+            (sb.SHARP_ALM2MAP, 0, alm0[:2], extra, g, a, 2, DP)]
+    ng, _ = sb.execute_batch(jobs)
+    assert ng == 5
+    r0 = [np.zeros(npix) for _ in range(nt)]
+    r2 = [np.zeros(npix) for _ in range(2 * nt)]
+    sb.execute(sb.SHARP_ALM2MAP, 0, [x.copy() for x in alm0], r0, g, a, nt, DP)
+    sb.execute(sb.SHARP_ALM2MAP, 2, [x.copy() for x in alm2], r2, g, a, nt, DP)
+    q0 = [np.zeros(nalm, np.complex128) for _ in range(nt)]
+    q2 = [np.zeros(nalm, np.complex128) for _ in range(2 * nt)]
+    sb.execute(sb.SHARP_MAP2ALM, 0, q0, [x.copy() for x in r0], g, a, nt, DP)
+    sb.execute(sb.SHARP_MAP2ALM, 2, q2, [x.copy() for x in r2], g, a, nt, DP)
+    for got, want in zip(m0 + m2 + o0 + o2, r0 + r2 + q0 + q2):
+        assert np.array_equal(got, want)
+    for got, want in zip(extra, r0[:2]):
+        assert rel_l2(got, want) < 1e-13
+    # independent jobs still merge across the list
+    outs = [np.zeros(npix) for _ in range(3)]
+    ng, _ = sb.execute_batch([(sb.SHARP_ALM2MAP, 0, [alm0[0]], [outs[0]], g, a, 1, DP),
+                              (sb.SHARP_MAP2ALM, 0, [q0[0].copy()], [r0[1].copy()], g, a, 1, DP),
+                              (sb.SHARP_ALM2MAP, 0, [alm0[2]], [outs[2]], g, a, 1, DP)])
+    assert ng == 2
+    assert rel_l2(outs[0], r0[0]) < 1e-13 and rel_l2(outs[2], r0[2]) < 1e-13

@@ -514,10 +514,12 @@ def test_register_bluestein_rings_match_reference(ref, spin, flags):
     # even rings whose half length has a large prime factor: Bluestein
     # convolution lengths 1024 (1018 = 2 * 509), 2048 (2004 = 4 * 3 * 167),
     # 4096 (2062 = 2 * 1031) and 8192 (4124 = 4 * 1031, the polar HEALPix
-    # form 4i); alias folding (lmax above half the shorter rings), phi0
-    # shifts, weights, an interleaved stride-2 pair, an unpaired ring and a
-    # pair of unequal lengths (which takes the size-class kernels); both
-    # directions, FP64 and single-precision I/O
+    # form 4i); long even rings of small factors that the register
+    # convolution takes as well (2400 = 2 * 1200, 6000 = 2 * 3000); alias
+    # folding (lmax above half the shorter rings), phi0 shifts, weights, an
+    # interleaved stride-2 pair, an unpaired ring and a pair of unequal
+    # lengths (which takes the size-class kernels); both directions, FP64
+    # and single-precision I/O
     rings = [  # (nph, theta, phi0, stride)
         (1018, 0.7, 0.1, 1), (1018, np.pi - 0.7, 0.1, 1),
         (2004, 0.9, 0.0, 1), (2004, np.pi - 0.9, 0.0, 1),
@@ -526,6 +528,8 @@ def test_register_bluestein_rings_match_reference(ref, spin, flags):
         (1018, 1.45, 0.2, 2), (1018, np.pi - 1.45, 0.2, 2),
         (2004, np.pi / 2, 0.4, 1),
         (1018, 0.5, 0.0, 1), (2004, np.pi - 0.5, 0.0, 1),
+        (2400, 0.35, 0.15, 1), (2400, np.pi - 0.35, 0.15, 1),
+        (6000, 0.25, 0.0, 1), (6000, np.pi - 0.25, 0.0, 1),
     ]
     nph = np.array([r[0] for r in rings], np.int32)
     theta = np.array([r[1] for r in rings])
