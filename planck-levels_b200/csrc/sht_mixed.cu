@@ -156,86 +156,132 @@ struct Shape {
 // Per-call image of the a_lm and coefficients: per (m, chunk) one block
 // [coefficients | B tile even | B tile odd], plus per-m epilogue constants
 // epi[m] = {scale[col], 2^31 * sum_even p[col], 2^31 * sum_odd p[col]}.
-// One CTA per m; warp w handles the columns col = w (mod 8).  The image is
-// zero-filled beforehand (padding rows and l > lmax stay zero).
+// One CTA per m.  A first pass over the m segment of A (rows read
+// contiguously, each thread on one component) finds the quantisation scale
+// of every column; then each chunk's block is assembled in shared memory
+// (the chunk's A rows staged there first; warp w forms the words of the
+// columns col = w (mod 8), lane = l within the chunk) and written out
+// whole with 16-byte stores, padding rows and l > lmax as zeros, so the
+// image needs no zero fill.
 // --------------------------------------------------------------------------
+template <class S>
 __global__ void __launch_bounds__(256)
-mixed_image_kernel(int lmax, int spin, int ncol, int ncomp, int NP, int CE, int BLK,
-                   const long long *__restrict__ moff, const double *__restrict__ ca,
-                   const double *__restrict__ cb, const double *__restrict__ cfac,
-                   const long long *__restrict__ ioff, const double2 *__restrict__ A, int ncA,
-                   int comp0, unsigned char *__restrict__ img, double *__restrict__ epi) {
+mixed_image_kernel(int lmax, int spin, const long long *__restrict__ moff,
+                   const double *__restrict__ ca, const double *__restrict__ cb,
+                   const double *__restrict__ cfac, const long long *__restrict__ ioff,
+                   const double2 *__restrict__ A, int ncA, int comp0,
+                   unsigned char *__restrict__ img, double *__restrict__ epi) {
+  constexpr int NCOL = S::NCOL, NCU = NCOL / 2;   // real columns, complex components
+  constexpr int G = 256 / NCU;                    // l-groups of the scale pass
+  constexpr int CPW = (NCOL + 7) / 8;             // columns per warp
+  __shared__ __align__(16) unsigned char blk[S::BLK];
+  __shared__ double2 arow[kMC][NCU];
+  __shared__ double red[G][NCOL];
+  __shared__ double inv[NCOL];
   const int m = blockIdx.x;
   const int lbase = max(m, spin);
   if (lbase > lmax) return;
   const long long mo = moff[m] - m;
   const int nch = (lmax - lbase + kMC) / kMC;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   unsigned char *base = img + ioff[m];
-  double *ep = epi + (long long)m * 3 * ncol;
+  double *ep = epi + (long long)m * 3 * NCOL;
   auto bound = [&](int l) { return spin == 0 ? sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) : 2.0; };
-  auto bval = [&](int l, int col) -> double {
-    const double c = cfac[mo + l];
-    if (c == 0.0) return 0.0;
-    const int j = col / (2 * ncomp), comp = (col >> 1) % ncomp;
-    const double2 a = A[(mo + l) * ncA + comp0 + ncomp * j + comp];
-    return ((col & 1) ? a.y : a.x) / c * bound(l);
+  // a_l * b_l of component c (both columns), zero where cfac is zero
+  auto scaled = [&](int l, int c) {
+    const double f = cfac[mo + l];
+    if (f == 0.0) return make_double2(0.0, 0.0);
+    const double2 a = A[(mo + l) * ncA + comp0 + c];
+    const double b = bound(l);
+    return make_double2(a.x / f * b, a.y / f * b);
   };
-  // coefficient blocks: (alpha_l, cq_l) or (a_l, b_l, cq_l, 0)
-  for (int e = threadIdx.x; e < nch * kMC; e += blockDim.x) {
-    const int l = lbase + e;
-    double *cf = reinterpret_cast<double *>(base + (long long)(e / kMC) * BLK) +
-                 (e % kMC) * (CE / 8);
-    const double cq = cfac[mo + l] * kQ / bound(l);
-    cf[0] = ca[mo + l];
-    if (spin == 0) {
-      cf[1] = cq;
-    } else {
-      cf[1] = cb[mo + l];
-      cf[2] = cq;
-      cf[3] = 0.0;
+  // ---- scale pass: column maxima ----
+  if (tid < G * NCU) {
+    const int c = tid % NCU, g = tid / NCU;
+    double mr = 0.0, mi = 0.0;
+    for (int l = lbase + g; l <= lmax; l += G) {
+      const double2 v = scaled(l, c);
+      mr = fmax(mr, fabs(v.x));
+      mi = fmax(mi, fabs(v.y));
     }
+    red[g][2 * c] = mr;
+    red[g][2 * c + 1] = mi;
   }
-  for (int col = warp; col < ncol; col += 8) {
+  __syncthreads();
+  if (tid < NCOL) {
     double amax = 0.0;
-    for (int l = lbase + lane; l <= lmax; l += 32) amax = fmax(amax, fabs(bval(l, col)));
+    for (int g = 0; g < G; ++g) amax = fmax(amax, red[g][tid]);
+    inv[tid] = amax > 0.0 ? kQ / amax : 0.0;
+    ep[tid] = amax / (kQ * kQ);
+  }
+  long long psum[CPW];
 #pragma unroll
-    for (int o = 16; o; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-    const double inv = amax > 0.0 ? kQ / amax : 0.0;
-    long long psum[2] = {0, 0};
-    for (int l = lbase + lane; l <= lmax; l += 32) {
-      const int p = static_cast<int>(llrint(bval(l, col) * inv));
-      // signed base-256 digits, each in [-128, 127]
-      int d[4], r = p;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        d[k] = ((r + 128) & 255) - 128;
-        r = (r - d[k]) >> 8;
-      }
-      d[3] = r;
-      const int ll = l - lbase;
-      psum[ll & 1] += p;
-      const int jj = (ll & (kMC - 1)) >> 1;
-      unsigned char *tile = base + (long long)(ll / kMC) * BLK + kMC * CE + (ll & 1) * NP * kKB;
-#pragma unroll
-      for (int w = 2; w <= 6; ++w) {
-        uint32_t word = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-          if (w - k >= 0 && w - k <= 3) word |= uint32_t(uint8_t(int8_t(d[w - k]))) << (8 * k);
-        const int row = col * kClasses + (w - 2);
-        *reinterpret_cast<uint32_t *>(tile + tile_off(row, 4 * jj)) = word;
+  for (int k = 0; k < CPW; ++k) psum[k] = 0;
+  // ---- blocks ----
+  for (int ch = 0; ch < nch; ++ch) {
+    const int l0 = lbase + ch * kMC;
+    for (int i = tid; i < S::BLK / 16; i += 256)
+      reinterpret_cast<uint4 *>(blk)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = tid; i < kMC * NCU; i += 256) {
+      const int r = i / NCU, c = i - r * NCU;
+      arow[r][c] = (l0 + r <= lmax) ? scaled(l0 + r, c) : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    // coefficient entries (alpha_l, cq_l) or (a_l, b_l, cq_l, 0)
+    if (tid < kMC) {
+      const int l = l0 + tid;
+      double *cf = reinterpret_cast<double *>(blk) + tid * (S::CE / 8);
+      const double cq = cfac[mo + l] * kQ / bound(l);
+      cf[0] = ca[mo + l];
+      if (spin == 0) {
+        cf[1] = cq;
+      } else {
+        cf[1] = cb[mo + l];
+        cf[2] = cq;
+        cf[3] = 0.0;
       }
     }
+    if (l0 + lane <= lmax) {
+      unsigned char *tile = blk + kMC * S::CE + (lane & 1) * S::NP * kKB;
+      const int jj = lane >> 1;
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+      for (int k = 0; k < CPW; ++k) {
+        const int col = warp + 8 * k;
+        if (col >= NCOL) break;
+        const double2 v = arow[lane][col >> 1];
+        const int p = static_cast<int>(llrint(((col & 1) ? v.y : v.x) * inv[col]));
+        // signed base-256 digits, each in [-128, 127]
+        int d[4], r = p;
 #pragma unroll
-      for (int o = 16; o; o >>= 1) psum[h] += __shfl_xor_sync(0xffffffffu, psum[h], o);
-    if (lane == 0) {
-      ep[col] = amax / (kQ * kQ);
-      ep[ncol + col] = 2147483648.0 * double(psum[0]);
-      ep[2 * ncol + col] = 2147483648.0 * double(psum[1]);
+        for (int q = 0; q < 3; ++q) {
+          d[q] = ((r + 128) & 255) - 128;
+          r = (r - d[q]) >> 8;
+        }
+        d[3] = r;
+        psum[k] += p;
+#pragma unroll
+        for (int w = 2; w <= 6; ++w) {
+          uint32_t word = 0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (w - q >= 0 && w - q <= 3) word |= uint32_t(uint8_t(int8_t(d[w - q]))) << (8 * q);
+          const int row = col * kClasses + (w - 2);
+          *reinterpret_cast<uint32_t *>(tile + tile_off(row, 4 * jj)) = word;
+        }
+      }
     }
+    __syncthreads();
+    uint4 *dst = reinterpret_cast<uint4 *>(base + (long long)ch * S::BLK);
+    for (int i = tid; i < S::BLK / 16; i += 256) dst[i] = reinterpret_cast<const uint4 *>(blk)[i];
+    __syncthreads();
+  }
+  // parity sums: lanes of equal parity (xor with even offsets keeps parity)
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) {
+    const int col = warp + 8 * k;
+#pragma unroll
+    for (int o = 16; o >= 2; o >>= 1) psum[k] += __shfl_xor_sync(0xffffffffu, psum[k], o);
+    if (col < NCOL && lane < 2) ep[(1 + lane) * NCOL + col] = 2147483648.0 * double(psum[k]);
   }
 }
 
@@ -574,13 +620,12 @@ void launch_shape(const JobDesc &job, const GeomPlan &gp, const CoefPlan &cp, co
   SHT_CUDA(::sht::ws_alloc(&epi, epi_bytes, st));
   SHT_CUDA(cudaMemcpyAsync(d_ioff, ioff.data(), sizeof(long long) * (mmax + 1),
                            cudaMemcpyHostToDevice, st));
-  SHT_CUDA(cudaMemsetAsync(img, 0, size_t(tot), st));
   SHT_CUDA(cudaMemsetAsync(epi, 0, epi_bytes, st));
   {
     ProfScope ps("mixed_image", st);
-    mixed_image_kernel<<<mmax + 1, 256, 0, st>>>(
-        lmax, spin, S::NCOL, S::NCOMP, S::NP, S::CE, S::BLK, cp.d_moff, cp.alpha, cp.beta,
-        cp.cfac, d_ioff, A, ncA, t0 * S::NCOMP, img, epi);
+    mixed_image_kernel<S><<<mmax + 1, 256, 0, st>>>(lmax, spin, cp.d_moff, cp.alpha, cp.beta,
+                                                    cp.cfac, d_ioff, A, ncA, t0 * S::NCOMP, img,
+                                                    epi);
     SHT_CUDA(cudaGetLastError());
   }
   {

@@ -1294,90 +1294,118 @@ __global__ void ring2phase_direct_kernel(const int *__restrict__ mlim, const int
 // sharp.c:547-606).  Staged values carry c_l (recurrence normalisation),
 // norm_l (spin > 0 / derivatives) and the real-harmonics m=0 factor.
 // ---------------------------------------------------------------------------
+// a_lm staging and scatter: one CTA per m moves the m segment between the
+// caller's arrays (l contiguous in each of the nalmptr arrays) and the rows
+// of A (the components of one l contiguous), through a shared-memory tile of
+// 2^lgtl l-values by nalmptr components (leading dimension nalmptr | 1, odd,
+// so both access patterns are free of bank conflicts).  Each side of the
+// copy is then coalesced: a warp reads or writes consecutive l of one array,
+// or consecutive components of one row.
 template <typename T>
-__global__ void stage_alm_kernel(int lmax, int nalmptr, const long long *__restrict__ mvstart,
-                                 long long astride, bool packed, long long alm_lo,
-                                 const long long *__restrict__ moff,
-                                 const double *__restrict__ cfac,
-                                 const double *__restrict__ norm_l, bool use_norm, double norm_m0,
-                                 const T *const *__restrict__ alm, double2 *__restrict__ A,
-                                 int ncA) {
+__global__ void __launch_bounds__(256)
+stage_alm_kernel(int lmax, int nalmptr, const long long *__restrict__ mvstart,
+                 long long astride, bool packed, long long alm_lo,
+                 const long long *__restrict__ moff, const double *__restrict__ cfac,
+                 const double *__restrict__ norm_l, bool use_norm, double norm_m0,
+                 const T *const *__restrict__ alm, double2 *__restrict__ A, int ncA, int lgtl) {
+  extern __shared__ double2 tile[];
+  const int tl = 1 << lgtl, ld = nalmptr | 1;
   const int m = blockIdx.x;
   const long long mo = moff[m] - m;
   const long long base = mvstart[m];
   const int nl = lmax - m + 1 + kPad;
-  for (int e = threadIdx.x; e < nl * nalmptr; e += blockDim.x) {
-    const int l = m + e / nalmptr;
-    const int c = e % nalmptr;
-    double2 v = make_double2(0.0, 0.0);
-    if (l <= lmax) {
-      const T *a = alm[c];
-      if (packed) {
-        if (m == 0) {
-          v.x = double(a[base + l * astride - alm_lo]);
+  for (int l0 = 0; l0 < nl; l0 += tl) {
+    for (int e = threadIdx.x; e < tl * nalmptr; e += blockDim.x) {
+      const int r = e & (tl - 1), c = e >> lgtl;
+      const int l = m + l0 + r;
+      double2 v = make_double2(0.0, 0.0);
+      if (l <= lmax) {
+        const T *a = alm[c];
+        if (packed) {
+          if (m == 0) {
+            v.x = double(a[base + l * astride - alm_lo]);
+          } else {
+            const long long ri = base + 2 * l * astride - alm_lo;
+            v = make_double2(double(a[ri]), double(a[ri + 1]));
+          }
         } else {
-          const long long ri = base + 2 * l * astride - alm_lo;
-          v = make_double2(double(a[ri]), double(a[ri + 1]));
+          const long long ri = 2 * (base + l * astride - alm_lo);
+          v.x = double(a[ri]);
+          v.y = (m == 0) ? 0.0 : double(a[ri + 1]);
         }
-      } else {
-        const long long ri = 2 * (base + l * astride - alm_lo);
-        v.x = double(a[ri]);
-        v.y = (m == 0) ? 0.0 : double(a[ri + 1]);
+        double f = cfac[mo + l];
+        if (use_norm) f *= norm_l[l];
+        if (m == 0) f *= norm_m0;
+        v = cscale(v, f);
       }
-      double f = cfac[mo + l];
-      if (use_norm) f *= norm_l[l];
-      if (m == 0) f *= norm_m0;
-      v = cscale(v, f);
+      tile[r * ld + c] = v;
     }
-    A[(mo + l) * ncA + c] = v;
+    __syncthreads();
+    for (int e = threadIdx.x; e < tl * nalmptr; e += blockDim.x) {
+      const int r = e / nalmptr, c = e - r * nalmptr;
+      if (l0 + r < nl) A[(mo + m + l0 + r) * ncA + c] = tile[r * ld + c];
+    }
+    __syncthreads();
   }
 }
 
 template <typename T>
-__global__ void scatter_alm_kernel(int lmax, int nalmptr, const long long *__restrict__ mvstart,
-                                   long long astride, bool packed, long long alm_lo,
-                                   const long long *__restrict__ moff,
-                                   const double *__restrict__ cfac,
-                                   const double *__restrict__ norm_l, bool use_norm,
-                                   double norm_m0, double sgn, bool add,
-                                   const double *__restrict__ Aout, int ncA,
-                                   T *const *__restrict__ alm) {
+__global__ void __launch_bounds__(256)
+scatter_alm_kernel(int lmax, int nalmptr, const long long *__restrict__ mvstart,
+                   long long astride, bool packed, long long alm_lo,
+                   const long long *__restrict__ moff, const double *__restrict__ cfac,
+                   const double *__restrict__ norm_l, bool use_norm, double norm_m0, double sgn,
+                   bool add, const double *__restrict__ Aout, int ncA,
+                   T *const *__restrict__ alm, int lgtl) {
+  extern __shared__ double2 tile[];
+  const int tl = 1 << lgtl, ld = nalmptr | 1;
   const int m = blockIdx.x;
   const long long mo = moff[m] - m;
   const long long base = mvstart[m];
   const int nl = lmax - m + 1;
-  for (int e = threadIdx.x; e < nl * nalmptr; e += blockDim.x) {
-    const int l = m + e / nalmptr;
-    const int c = e % nalmptr;
-    const double *src = Aout + ((mo + l) * ncA + c) * 2;
-    double f = cfac[mo + l] * sgn;
-    if (use_norm) f *= norm_l[l];
-    double vr = src[0] * f, vi = src[1] * f;
-    T *a = alm[c];
-    if (m == 0) {
-      vr *= norm_m0;
-      if (packed) {
-        T *px = a + (base + l * astride - alm_lo);
-        *px = add ? T(*px + T(vr)) : T(vr);
+  const double2 *src = reinterpret_cast<const double2 *>(Aout);
+  for (int l0 = 0; l0 < nl; l0 += tl) {
+    for (int e = threadIdx.x; e < tl * nalmptr; e += blockDim.x) {
+      const int r = e / nalmptr, c = e - r * nalmptr;
+      if (l0 + r < nl) tile[r * ld + c] = src[(mo + m + l0 + r) * ncA + c];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < tl * nalmptr; e += blockDim.x) {
+      const int r = e & (tl - 1), c = e >> lgtl;
+      if (l0 + r >= nl) continue;
+      const int l = m + l0 + r;
+      const double2 v = tile[r * ld + c];
+      double f = cfac[mo + l] * sgn;
+      if (use_norm) f *= norm_l[l];
+      double vr = v.x * f, vi = v.y * f;
+      T *a = alm[c];
+      if (m == 0) {
+        vr *= norm_m0;
+        if (packed) {
+          T *px = a + (base + l * astride - alm_lo);
+          *px = add ? T(*px + T(vr)) : T(vr);
+        } else {
+          T *px = a + 2 * (base + l * astride - alm_lo);
+          if (add) {
+            px[0] += T(vr);
+          } else {
+            px[0] = T(vr);
+            px[1] = T(0);
+          }
+        }
       } else {
-        T *px = a + 2 * (base + l * astride - alm_lo);
+        T *px = packed ? a + (base + 2 * l * astride - alm_lo)
+                       : a + 2 * (base + l * astride - alm_lo);
         if (add) {
           px[0] += T(vr);
+          px[1] += T(vi);
         } else {
           px[0] = T(vr);
-          px[1] = T(0);
+          px[1] = T(vi);
         }
       }
-    } else {
-      T *px = packed ? a + (base + 2 * l * astride - alm_lo) : a + 2 * (base + l * astride - alm_lo);
-      if (add) {
-        px[0] += T(vr);
-        px[1] += T(vi);
-      } else {
-        px[0] = T(vr);
-        px[1] = T(vi);
-      }
     }
+    __syncthreads();
   }
 }
 
@@ -1737,21 +1765,35 @@ void launch_ring2phase_direct(const JobDesc &job, const GeomPlan &gp, long long 
   SHT_CUDA(cudaGetLastError());
 }
 
+// log2 of the staging tile's l extent: at least 32 l-values (a warp's
+// worth of one array) and about 512 entries per tile (few components: more
+// l-values, so the 256 threads stay busy), at most 256, and no more than
+// 48 KiB of shared memory (nalmptr | 1 entries per l).
+static int stage_tile_lg(int nalmptr) {
+  const size_t ld = size_t(nalmptr | 1);
+  int lg = 5;
+  while (lg < 8 && (2 << lg) * nalmptr <= 512) ++lg;
+  while (lg > 0 && (sizeof(double2) << lg) * ld > 48 * 1024) --lg;
+  return lg;
+}
+
 void launch_stage_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
                       const CoefPlan &cp, const double *norm_l, const void *const *alm_dev,
                       int nalmptr, double2 *A, int ncA, cudaStream_t st) {
   const bool use_norm = job.spin > 0 || job.type == SHARP_ALM2MAP_DERIV1;
   const double norm_m0 = (job.flags & SHARP_REAL_HARMONICS) ? kSqrtTwo : 1.0;
   const int blocks = job.mmax + 1;
+  const int lg = stage_tile_lg(nalmptr);
+  const size_t smem = (sizeof(double2) << lg) * size_t(nalmptr | 1);
   ProfScope ps("stage_alm", st);
   if (job.dp)
-    stage_alm_kernel<double><<<blocks, 256, 0, st>>>(
+    stage_alm_kernel<double><<<blocks, 256, smem, st>>>(
         job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
-        use_norm, norm_m0, reinterpret_cast<const double *const *>(alm_dev), A, ncA);
+        use_norm, norm_m0, reinterpret_cast<const double *const *>(alm_dev), A, ncA, lg);
   else
-    stage_alm_kernel<float><<<blocks, 256, 0, st>>>(
+    stage_alm_kernel<float><<<blocks, 256, smem, st>>>(
         job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
-        use_norm, norm_m0, reinterpret_cast<const float *const *>(alm_dev), A, ncA);
+        use_norm, norm_m0, reinterpret_cast<const float *const *>(alm_dev), A, ncA, lg);
   SHT_CUDA(cudaGetLastError());
 }
 
@@ -1764,15 +1806,17 @@ void launch_scatter_alm(const JobDesc &job, const AlmPlan &ap, long long alm_lo,
   const double sgn = (job.flags & SHARP_SUBTRACT) ? -1.0 : 1.0;
   const bool add = (job.flags & (SHARP_ADD | SHARP_SUBTRACT)) != 0;
   const int blocks = job.mmax + 1;
+  const int lg = stage_tile_lg(nalmptr);
+  const size_t smem = (sizeof(double2) << lg) * size_t(nalmptr | 1);
   ProfScope ps("scatter_alm", st);
   if (job.dp)
-    scatter_alm_kernel<double><<<blocks, 256, 0, st>>>(
+    scatter_alm_kernel<double><<<blocks, 256, smem, st>>>(
         job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
-        use_norm, norm_m0, sgn, add, Aout, ncA, reinterpret_cast<double *const *>(alm_dev));
+        use_norm, norm_m0, sgn, add, Aout, ncA, reinterpret_cast<double *const *>(alm_dev), lg);
   else
-    scatter_alm_kernel<float><<<blocks, 256, 0, st>>>(
+    scatter_alm_kernel<float><<<blocks, 256, smem, st>>>(
         job.lmax, nalmptr, ap.mvstart, ap.stride, ap.packed, alm_lo, cp.d_moff, cp.cfac, norm_l,
-        use_norm, norm_m0, sgn, add, Aout, ncA, reinterpret_cast<float *const *>(alm_dev));
+        use_norm, norm_m0, sgn, add, Aout, ncA, reinterpret_cast<float *const *>(alm_dev), lg);
   SHT_CUDA(cudaGetLastError());
 }
 
