@@ -751,6 +751,30 @@ __device__ __forceinline__ void dft16(double2 (&v)[16]) {
 // twiddles W_len^(k0 f) from a table W of exp(-2 pi i j/tl), j < tl (a
 // multiple of len), so W_len^e = W[(tl/len) e].
 // Inputs i >= NIN are taken as zero (not read).
+// The arithmetic and stores of a pass on inputs already in registers: v[i]
+// is the entry at base + s i (s = len/16, base = (u/s) len + k0, k0 = u mod s).
+template <int N, bool INV>
+__device__ __forceinline__ void pw_pass16_regs(double2 (&v)[16], double2 *buf, int len,
+                                               const double2 *__restrict__ W, int tl) {
+  const int s = len >> 4;
+  const int u = threadIdx.x;
+  const int k0 = u & (s - 1);
+  const int base = (u / s) * len + k0;
+  dft16<INV>(v);
+  if (s > 1 && k0 > 0) {
+    double2 w1 = __ldg(W + (tl / len) * k0);
+    if (INV) w1.y = -w1.y;
+    double2 w = w1;
+#pragma unroll
+    for (int f = 1; f < 16; ++f) {
+      v[f] = cmul(v[f], w);
+      if (f < 15) w = cmul(w, w1);
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 16; ++f) buf[pw_pad(base + s * f)] = v[f];
+}
+
 template <int N, bool INV, int NIN = 16>
 __device__ __forceinline__ void pw_pass16(double2 *buf, int len, const double2 *__restrict__ W,
                                           int tl) {
@@ -789,6 +813,24 @@ __device__ __forceinline__ void pw_pass_last(double2 *buf) {
     small_dft<R>(v, INV);
 #pragma unroll
     for (int i = 0; i < R; ++i) buf[pw_pad(b * R + i)] = v[i];
+  }
+}
+
+// The passes of pw_fft after the first (which the caller ran from registers
+// with pw_pass16_regs and a __syncthreads).
+template <int N, bool INV>
+__device__ void pw_fft_rest(double2 *buf, const double2 *__restrict__ W, int tl) {
+  int len = N >> 4;
+#pragma unroll
+  for (int q = 1; q < pw_passes16(N); ++q) {
+    pw_pass16<N, INV>(buf, len, W, tl);
+    __syncthreads();
+    len >>= 4;
+  }
+  constexpr int RL = pw_last(N);
+  if constexpr (RL > 1) {
+    pw_pass_last<N, RL, INV>(buf);
+    __syncthreads();
   }
 }
 
@@ -854,7 +896,9 @@ __device__ __forceinline__ int pw_pos(int k) {
 
 // phase -> ring.  Grid: (2 * pairs of this length, components).
 template <typename T, int N>
-__global__ void __launch_bounds__(N / 16)
+// (three CTAs per SM at N = 4096: 80 registers, a few spilled; measured
+// 8.9 against 9.5 ms per 12-transform synthesis at Nside 2048)
+__global__ void __launch_bounds__(N / 16, (N == 4096 ? 3 : 1))
 phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
                        const int *__restrict__ nph, const long long *__restrict__ ofs,
                        const double *__restrict__ phi0, const double *__restrict__ weight,
@@ -888,8 +932,11 @@ phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     if (rot) t = cmul(t, shift_of(slo, shi, m));
     return t;
   };
-  // Z_k = (C_k + conj C_{N-k}) + i conj(W^k) (C_k - conj C_{N-k}), k < N
-#pragma unroll 4
+  // Z_k = (C_k + conj C_{N-k}) + i conj(W^k) (C_k - conj C_{N-k}), k < N,
+  // for k = tid + (N/16) i: exactly this thread's inputs of the first pass,
+  // which therefore runs from registers
+  double2 v[16];
+#pragma unroll
   for (int i = 0; i < 16; ++i) {
     const int k = threadIdx.x + (N / 16) * i;
     double2 ck = tm(k), cn;
@@ -904,10 +951,11 @@ phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     const double2 sm = cadd(ck, cn), df = csub(ck, cn);
     const double2 w = __ldg(W + k);
     const double2 iw = make_double2(w.y, w.x);   // i * conj(w)
-    buf[pw_pad(k)] = cadd(sm, cmul(iw, df));
+    v[i] = cadd(sm, cmul(iw, df));
   }
+  pw_pass16_regs<N, true>(v, buf, N, W, 2 * N);
   __syncthreads();
-  pw_fft<N, true>(buf, W, 2 * N);
+  pw_fft_rest<N, true>(buf, W, 2 * N);
   // pixels 2j, 2j+1 = Re, Im z_j
   T *map = maps[c] + (ofs[ring] - map_lo);
 #pragma unroll 4
@@ -945,13 +993,17 @@ ring2phase_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   const double2 *W = twiddle + fdesc[fftidx[ring]].tw;
   const T *map = maps[c] + (ofs[ring] - map_lo);
   if (rot) build_shift(slo, shi, mm, -ph);
-#pragma unroll 4
+  // pixels 2j, 2j+1 for j = tid + (N/16) s2: this thread's inputs of the
+  // first pass, which runs from registers
+  double2 v[16];
+#pragma unroll
   for (int s2 = 0; s2 < 16; ++s2) {
     const int j = threadIdx.x + (N / 16) * s2;
-    buf[pw_pad(j)] = make_double2(double(map[2 * j]), double(map[2 * j + 1]));
+    v[s2] = make_double2(double(map[2 * j]), double(map[2 * j + 1]));
   }
+  pw_pass16_regs<N, false>(v, buf, N, W, 2 * N);
   __syncthreads();
-  pw_fft<N, false>(buf, W, 2 * N);
+  pw_fft_rest<N, false>(buf, W, 2 * N);
   // X_k = (Z_k + conj Z_{N-k})/2 - i W^k (Z_k - conj Z_{N-k})/2, k <= N;
   // phase_m = X_m wgt e^{-i m phi0} for m <= mm (<= N: no folding)
   double2 *dst = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
@@ -996,16 +1048,18 @@ __device__ __forceinline__ double2 pb_chirp(const double2 *__restrict__ W, int j
 
 // In place: natural-order input (upper half zero) -> M times the cyclic
 // convolution with b, natural order, lower half.  W: exp(-2 pi i j/tl).
+// The callers run the first forward pass themselves from registers
+// (pw_pass16_regs on the entries tid + (M/16) i, i < 8, the rest zero,
+// then a __syncthreads); this runs the rest.
 template <int M>
 __device__ void pb_convolve(double2 *buf, const double2 *__restrict__ W, int tl,
                             const double2 *__restrict__ bh) {
   constexpr int P16 = pw_passes16(M), RL = pw_last(M);
   constexpr int FWD = (RL > 1) ? P16 : P16 - 1;   // radix-16 passes before the product
-  int len = M;
+  int len = M >> 4;
 #pragma unroll
-  for (int q = 0; q < FWD; ++q) {
-    if (q == 0) pw_pass16<M, false, 8>(buf, len, W, tl);
-    else pw_pass16<M, false>(buf, len, W, tl);
+  for (int q = 1; q < FWD; ++q) {
+    pw_pass16<M, false>(buf, len, W, tl);
     __syncthreads();
     len >>= 4;
   }
@@ -1123,23 +1177,25 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     buf[pw_pad(k)] = acc;
   }
   __syncthreads();
-  // Z_k = (C_k + conj C_{N-k}) + i conj(W^k) (C_k - conj C_{N-k}), k < N,
-  // conjugated and times c_k; zero padding on [N, M/2)
-  auto zin = [&](double2 ck, double2 cn, int k) {
-    cn = cconj(cn);
-    const double2 sm = cadd(ck, cn), df = csub(ck, cn);
-    const double2 w = __ldg(W + k);
-    const double2 iw = make_double2(w.y, w.x);   // i * conj(w)
-    return cmul(cconj(cadd(sm, cmul(iw, df))), pb_chirp(W, k, n));
-  };
-  for (int k = threadIdx.x; 2 * k <= N; k += NT) {
-    const int kk = N - k;
-    const double2 ck = buf[pw_pad(k)], cn = buf[pw_pad(kk)];
-    buf[pw_pad(k)] = zin(ck, cn, k);
-    if (k == 0) buf[pw_pad(N)] = make_double2(0.0, 0.0);
-    else if (kk != k) buf[pw_pad(kk)] = zin(cn, ck, kk);
+  // x_k = conj(Z_k) c_k with Z_k = (C_k + conj C_{N-k}) + i conj(W^k)
+  // (C_k - conj C_{N-k}) for k < N, zero on [N, M/2): for k = tid + NT i,
+  // i < 8, this thread's inputs of the first forward pass, which runs from
+  // registers once every thread has read its C values
+  double2 v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int k = threadIdx.x + NT * i;
+    v[i] = make_double2(0.0, 0.0);
+    if (i < 8 && k < N) {
+      const double2 ck = buf[pw_pad(k)], cn = cconj(buf[pw_pad(N - k)]);
+      const double2 sm = cadd(ck, cn), df = csub(ck, cn);
+      const double2 w = __ldg(W + k);
+      const double2 iw = make_double2(w.y, w.x);   // i * conj(w)
+      v[i] = cmul(cconj(cadd(sm, cmul(iw, df))), pb_chirp(W, k, n));
+    }
   }
-  for (int j = N + 1 + threadIdx.x; j < M / 2; j += NT) buf[pw_pad(j)] = make_double2(0.0, 0.0);
+  __syncthreads();
+  pw_pass16_regs<M, false>(v, buf, M, wpow2, P);
   __syncthreads();
   pb_convolve<M>(buf, wpow2, P, bh);
   // z_j = conj(c_j conv_j): pixels 2j, 2j+1 = Re, Im z_j
@@ -1186,14 +1242,18 @@ ring2phase_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   const T *map = maps[c] + (ofs[ring] - map_lo);
   const long long st = stride[ring];
   if (rot) build_shift(slo, shi, mm, -ph);
-  // x_j c_j, x_j = pixels 2j + i (2j+1); zero padding on [N, M/2)
-  for (int j = threadIdx.x; j < M / 2; j += NT) {
-    double2 x = make_double2(0.0, 0.0);
-    if (j < N)
-      x = cmul(make_double2(double(map[(2 * j) * st]), double(map[(2 * j + 1) * st])),
-               pb_chirp(W, j, n));
-    buf[pw_pad(j)] = x;
+  // x_j c_j, x_j = pixels 2j + i (2j+1), zero on [N, M): for j = tid + NT i
+  // this thread's inputs of the first forward pass, run from registers
+  double2 v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int j = threadIdx.x + NT * i;
+    v[i] = make_double2(0.0, 0.0);
+    if (i < 8 && j < N)
+      v[i] = cmul(make_double2(double(map[(2 * j) * st]), double(map[(2 * j + 1) * st])),
+                  pb_chirp(W, j, n));
   }
+  pw_pass16_regs<M, false>(v, buf, M, wpow2, P);
   __syncthreads();
   pb_convolve<M>(buf, wpow2, P, bh);
   // Z_k = c_k conv_k (Z_N = Z_0);
