@@ -124,30 +124,6 @@ template <int N>
 __device__ __forceinline__ void named_sync(int id) {
   asm volatile("bar.sync %0, %1;" :: "r"(id), "n"(N) : "memory");
 }
-// 16 consecutive 32-bit columns of this thread's TMEM lane (store)
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
-      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
-      :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]),
-         "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]),
-         "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
-}
-__device__ __forceinline__ void tmem_st_wait() {
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-// D[tmem] (+)= A(tmem) * B(smem)^T, kind::i8 (A signed, B unsigned), int32.
-__device__ __forceinline__ void mma_i8_tmem_a(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
-                                              uint32_t idesc, uint32_t accumulate) {
-  const uint32_t z = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      :: "r"(d_tmem), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z),
-         "r"(z), "r"(z)
-      : "memory");
-}
 // Instruction descriptor: D s32, A s8, B u8, both K-major, M = m, N = n.
 __host__ __device__ constexpr uint32_t make_idesc_s8u8(int m, int n) {
   return (2u << 4) | (1u << 7) | (0u << 10) | (uint32_t(n >> 3) << 17) |
