@@ -155,7 +155,7 @@ int sharp_b200_execute_batch (const sharp_b200_job *jobs, int njobs,
    sharp_b200_last_error() says how much scratch they would need.  Other
    failures follow the library's abort policy (in non-abort mode: -1).
    Returns 0 on success.  The first call on each device looks up the array's
-   address (make it before any stream capture).  All calls share the array:
+   address.  All calls share the array:
    calls that overlap on the GPU race and must be serialised by the caller. */
 int sharp_b200_alm2map_noalloc (const sharp_geom_info *geom_info,
   const sharp_alm_info *alm_info, const void *alm, void *map, void *stream);

@@ -13,8 +13,8 @@
 // rebuilt on every call.
 //
 // The symbol address of the array is looked up once per device, on the first
-// call made with that device current (cudaGetSymbolAddress); that first call
-// should come before any stream capture.  All calls share the one array:
+// call made with that device current (cudaGetSymbolAddress).  All calls share
+// the one array:
 // calls that overlap on the GPU (different streams, or host threads calling
 // concurrently) race on it and must be serialised by the caller.  Each call
 // rewrites every part of the array it reads before reading it, so the
