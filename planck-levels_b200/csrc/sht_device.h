@@ -67,10 +67,11 @@ struct GeomHost {
   bool map_covered = false;
 };
 // Shared memory of the register ring kernels (pw_entries(N) buffer entries
-// of the ring kernels plus the phi0 rotation slices), in double2 entries.
+// of the ring kernels, the phi0 rotation slices and the twiddle slices of
+// the power-of-two analysis), in double2 entries.
 inline size_t pow2_ring_smem_entries(int N, int mmax) {
   const int n = N - 1;
-  return size_t(n + (n >> 4) + (n >> 8) + 1) + 64 + mmax / 64 + 2;
+  return size_t(n + (n >> 4) + (n >> 8) + 1) + 64 + mmax / 64 + 2 + 64 + N / 64 + 1;
 }
 constexpr size_t kRingSmemLimit = 227 * 1024;
 // Complex FFT length N of a ring that the power-of-two ring kernels take

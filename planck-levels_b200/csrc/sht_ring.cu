@@ -26,6 +26,7 @@
 #include <cmath>
 
 #include "sht_device.h"
+#include "sht_tc.cuh"   // mbarriers and bulk copies
 
 namespace sht {
 
@@ -894,11 +895,16 @@ __device__ __forceinline__ int pw_pos(int k) {
   return p + rem;   // the last digit (radix pw_last(N)) has stride 1
 }
 
+// CTAs per SM the synthesis kernel is compiled for: three at N = 4096 (80
+// registers, a few spilled; measured 8.9 against 9.5 ms per 12-transform
+// synthesis at Nside 2048 with two), 128 registers for the shorter rings
+__host__ __device__ constexpr int pow2_synth_min_blocks(int N) {
+  return N == 4096 ? 3 : N == 2048 ? 4 : N == 1024 ? 8 : 1;
+}
+
 // phase -> ring.  Grid: (2 * pairs of this length, components).
 template <typename T, int N>
-// (three CTAs per SM at N = 4096: 80 registers, a few spilled; measured
-// 8.9 against 9.5 ms per 12-transform synthesis at Nside 2048)
-__global__ void __launch_bounds__(N / 16, (N == 4096 ? 3 : 1))
+__global__ void __launch_bounds__(N / 16, pow2_synth_min_blocks(N))
 phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
                        const int *__restrict__ nph, const long long *__restrict__ ofs,
                        const double *__restrict__ phi0, const double *__restrict__ weight,
@@ -907,9 +913,15 @@ phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
                        int ncm, int mmax, int flags, T *const *__restrict__ maps,
                        long long map_lo) {
   extern __shared__ double2 smem[];
+  __shared__ uint64_t row_full;
   double2 *buf = smem;
   double2 *slo = smem + pw_entries(N);
   double2 *shi = slo + kShiftLo;
+  // while the Z_k are formed the buffer holds the phase row (entries 0 .. mm
+  // <= N) and, behind it where there is room (N >= 2048), the twiddle slices
+  // W^k = twh[k / 64] twl[k mod 64], k < N
+  constexpr bool kSlices = N + 1 + kTwLo + N / kTwLo <= pw_entries(N);
+  double2 *twl = buf + (N + 1), *twh = twl + kTwLo;
   const int p = pairs[blockIdx.x >> 1], h = blockIdx.x & 1, c = blockIdx.y;
   const int ring = 2 * p + h;
   if (nph[ring] <= 0) return;        // unpaired ring: nothing in this hemisphere
@@ -923,12 +935,31 @@ phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   const bool rot = fabs(ph) >= 1e-14;
   const double2 *W = twiddle + fdesc[fftidx[ring]].tw;
   const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
-  if (rot) build_shift(slo, shi, mm, ph);
+  // the phase row into shared memory by one bulk copy (16-byte aligned, a
+  // multiple of 16 bytes), while the threads build the twiddle and phi0
+  // slices
+  if (threadIdx.x == 0) {
+    mbar_init(&row_full, 1);
+    fence_mbar_init();
+  }
   __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_tx(&row_full, uint32_t(16 * (mm + 1)));
+    bulk_g2s(buf, src, uint32_t(16 * (mm + 1)), &row_full);
+  }
+  if constexpr (kSlices) load_twshared(twl, twh, W, N);   // W: the table of 2N entries
+  if (rot) build_shift(slo, shi, mm, ph);
+  // a copy that did not complete within the bounded wait is redone by the
+  // threads from global memory (the same values, so a late bulk write
+  // changes nothing)
+  if (__syncthreads_or(!mbar_wait(&row_full, 0))) {
+    for (int m = threadIdx.x; m <= mm; m += N / 16) buf[m] = src[m];
+    __syncthreads();
+  }
   // t_m = phase_m wgt e^{i m phi0} (zero above mm); C_0 and C_N real
   auto tm = [&](int m) {
     if (m > mm) return make_double2(0.0, 0.0);
-    double2 t = cscale(src[m], wgt);
+    double2 t = cscale(buf[m], wgt);
     if (rot) t = cmul(t, shift_of(slo, shi, m));
     return t;
   };
@@ -949,10 +980,11 @@ phase2ring_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     }
     cn = cconj(cn);
     const double2 sm = cadd(ck, cn), df = csub(ck, cn);
-    const double2 w = __ldg(W + k);
+    const double2 w = kSlices ? cmul(twh[k >> 6], twl[k & (kTwLo - 1)]) : __ldg(W + k);
     const double2 iw = make_double2(w.y, w.x);   // i * conj(w)
     v[i] = cadd(sm, cmul(iw, df));
   }
+  __syncthreads();   // the row and the slices are read; the first pass overwrites them
   pw_pass16_regs<N, true>(v, buf, N, W, 2 * N);
   __syncthreads();
   pw_fft_rest<N, true>(buf, W, 2 * N);
@@ -981,6 +1013,8 @@ ring2phase_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   double2 *buf = smem;
   double2 *slo = smem + pw_entries(N);
   double2 *shi = slo + kShiftLo;
+  // twiddle slices for the unpacking: W^k = twh[k / 64] twl[k mod 64], k <= N
+  double2 *twl = shi + (mmax / kShiftLo + 2), *twh = twl + kTwLo;
   const int p = pairs[blockIdx.x >> 1], h = blockIdx.x & 1, c = blockIdx.y;
   const int ring = 2 * p + h;
   if (nph[ring] <= 0) return;
@@ -993,6 +1027,7 @@ ring2phase_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   const double2 *W = twiddle + fdesc[fftidx[ring]].tw;
   const T *map = maps[c] + (ofs[ring] - map_lo);
   if (rot) build_shift(slo, shi, mm, -ph);
+  load_twshared(twl, twh, W, N + 1);   // W: the table of 2N entries
   // pixels 2j, 2j+1 for j = tid + (N/16) s2: this thread's inputs of the
   // first pass, which runs from registers
   double2 v[16];
@@ -1011,7 +1046,7 @@ ring2phase_pow2_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     const double2 zk = buf[pw_pad(pw_pos<N>(k == N ? 0 : k))];
     const double2 zn = cconj(buf[pw_pad(pw_pos<N>(k == 0 ? 0 : N - k))]);
     const double2 sm = cadd(zk, zn), df = csub(zk, zn);
-    const double2 w = __ldg(W + k);
+    const double2 w = cmul(twh[k >> 6], twl[k & (kTwLo - 1)]);
     const double2 mi_w = make_double2(w.y, -w.x);  // -i * w
     double2 xk = cscale(cadd(sm, cmul(mi_w, df)), 0.5);
     if (k == 0 || k == N) xk.y = 0.0;
@@ -1670,7 +1705,8 @@ void ring2phase_pow2(const JobDesc &job, const GeomPlan &gp, int cls, long long 
                      const void *const *maps_dev, int nmapptr, double2 *phase, int ncm,
                      cudaStream_t st) {
   auto k = ring2phase_pow2_kernel<T, N>;
-  const size_t smem = pow2_smem(N, job.mmax);
+  // plus the twiddle slices of the unpacking
+  const size_t smem = pow2_smem(N, job.mmax) + sizeof(double2) * (kTwLo + N / kTwLo + 1);
   SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   k<<<dim3(2 * gp.pw_count[cls], nmapptr), N / 16, smem, st>>>(
       gp.pw_pairs + gp.pw_start[cls], gp.mlim, gp.nph, gp.ofs, gp.phi0, gp.weight, gp.fft,
