@@ -36,6 +36,8 @@ struct FftDesc {
                     // radix-4 stages (/M), or -1 when no generic-class ring uses it
   long long bhat2;  // the same in the digit order of the radix-16 register passes,
                     // or -1 when no register-Bluestein ring uses it
+  long long chirp;  // with bhat2: offset of c_j = exp(-pi i j^2/N), j < N, in natural
+                    // order (the register kernels read it coalesced), else -1
 };
 
 // Host half of a geometry plan (build_geom_host, no device calls): what the
@@ -55,7 +57,7 @@ struct GeomHost {
   std::vector<int> tw_n, tw_off;      // per distinct length: n and table offset
   std::vector<int> blue_idx;          // descriptors with a radix-4 chirp transform (bhat)
   std::vector<int> blue2_idx;         // descriptors with a register-pass one (bhat2)
-  long long tw_total = 0, bhat_total = 0;
+  long long tw_total = 0, bhat_total = 0, chirp_total = 0;
   std::vector<int> cls_N, cls_start, cls_count, cls_bufA, cls_bufB, cls_pairs;
   // pairs whose rings run the power-of-two register FFT (pow2_ring_length):
   // complex length pw_N[c], listed at pw_pairs[pw_start[c] .. +pw_count[c])
@@ -120,6 +122,7 @@ struct GeomPlan {
   FftDesc *fdesc = nullptr;
   double2 *twiddle = nullptr;
   double2 *bhat = nullptr;           // Bluestein chirp transforms
+  double2 *chirp = nullptr;          // chirps of the register Bluestein lengths
   double2 *wpow2 = nullptr;          // exp(-2 pi i j/P), j<P, P = largest M
   int P = 2;
   // ring FFT size classes: pairs whose largest complex FFT length is

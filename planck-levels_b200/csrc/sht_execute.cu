@@ -234,7 +234,7 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
         const long long blue_cost = 2ll * ((long long)M * lg + 2ll * d.N);
         d.blue = (d.N > 16 && blue_cost < direct) ? 1 : 0;
         d.M = M;   // the convolution length, also for rings the register Bluestein takes
-        d.bhat = d.bhat2 = -1;
+        d.bhat = d.bhat2 = d.chirp = -1;
         h.tw_n.push_back(d.n);
         h.tw_off.push_back(int(h.tw_total));
         h.tw_total += d.n;
@@ -363,6 +363,8 @@ GeomHost build_geom_host(const sharp_geom_info *g, int lmax, int mmax, int spin)
     if (use16[i]) {
       d.bhat2 = h.bhat_total;
       h.bhat_total += d.M;
+      d.chirp = h.chirp_total;
+      h.chirp_total += d.N;
       h.blue2_idx.push_back(i);
     }
     if (use4[i] || use16[i]) h.P = std::max(h.P, d.M);
@@ -427,6 +429,7 @@ std::unique_ptr<GeomPlan> build_geom_plan(const sharp_geom_info *g, int lmax, in
   launch_twiddles(*gp, int(h.tw_total), h.tw_n, h.tw_off, st);
   SHT_CUDA(cudaMalloc(&gp->bhat, sizeof(double2) * std::max<long long>(h.bhat_total, 1)));
   SHT_CUDA(cudaMalloc(&gp->wpow2, sizeof(double2) * gp->P));
+  SHT_CUDA(cudaMalloc(&gp->chirp, sizeof(double2) * std::max<long long>(h.chirp_total, 1)));
   launch_bluestein_setup(*gp, h, st);
   SHT_CUDA(cudaStreamSynchronize(st));
   return gp;
@@ -1302,7 +1305,7 @@ GeomPlan::~GeomPlan() {
   dev_free(phi0); dev_free(weight); dev_free(ofs); dev_free(nph); dev_free(stride);
   dev_free(fft); dev_free(fdesc); dev_free(twiddle); dev_free(cls_pairs); dev_free(pw_pairs);
   dev_free(pb_pairs);
-  dev_free(bhat); dev_free(wpow2);
+  dev_free(bhat); dev_free(wpow2); dev_free(chirp);
 }
 CoefPlan::~CoefPlan() {
   dev_free(d_moff); dev_free(alpha); dev_free(beta); dev_free(cfac); dev_free(seed);

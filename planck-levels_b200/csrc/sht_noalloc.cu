@@ -133,6 +133,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   const size_t o_tw = L.take<double2>(h.tw_total);
   const size_t o_wp = L.take<double2>(h.P);
   const size_t o_bhat = L.take<double2>(h.bhat_total);
+  const size_t o_chirp = L.take<double2>(h.chirp_total);
   const size_t o_moff = L.take<long long>(mmax + 2);
   const size_t o_alpha = L.take<double>(off), o_cfac = L.take<double>(off);
   const size_t o_mfac = L.take<double>(mmax + 1);
@@ -191,7 +192,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
     ~Release() {
       g.cth = g.sth = nullptr; g.mlim = g.count = nullptr; g.items = nullptr;
       g.phi0 = g.weight = nullptr; g.ofs = nullptr; g.nph = g.stride = g.fft = nullptr;
-      g.fdesc = nullptr; g.twiddle = g.bhat = g.wpow2 = nullptr; g.cls_pairs = nullptr;
+      g.fdesc = nullptr; g.twiddle = g.bhat = g.wpow2 = g.chirp = nullptr; g.cls_pairs = nullptr;
       g.pw_pairs = nullptr; g.pb_pairs = nullptr;
       c.d_moff = nullptr; c.alpha = c.beta = c.cfac = c.seed = nullptr; c.seed_exp = nullptr;
       a.mvstart = nullptr;
@@ -209,6 +210,7 @@ int alm2map_noalloc(const sharp_geom_info *g, const sharp_alm_info *a, const voi
   gp.fft = static_cast<int *>(at(o_fft)); gp.fdesc = static_cast<FftDesc *>(at(o_fdesc));
   gp.twiddle = static_cast<double2 *>(at(o_tw)); gp.wpow2 = static_cast<double2 *>(at(o_wp));
   gp.bhat = static_cast<double2 *>(at(o_bhat)); gp.P = h.P;
+  gp.chirp = static_cast<double2 *>(at(o_chirp));
   gp.cls_N = h.cls_N; gp.cls_start = h.cls_start; gp.cls_count = h.cls_count;
   gp.cls_bufA = h.cls_bufA; gp.cls_bufB = h.cls_bufB;
   gp.cls_pairs = static_cast<int *>(at(o_cls));

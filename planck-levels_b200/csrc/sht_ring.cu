@@ -1144,13 +1144,14 @@ __global__ void __launch_bounds__(M / 16)
 bluestein_pw_setup_kernel(const FftDesc *__restrict__ fdesc, const int *__restrict__ blue2_idx,
                           const double2 *__restrict__ twiddle,
                           const double2 *__restrict__ wpow2, int P,
-                          double2 *__restrict__ bhat) {
+                          double2 *__restrict__ bhat, double2 *__restrict__ chirp) {
   extern __shared__ double2 smem[];
   const FftDesc &d = fdesc[blue2_idx[blockIdx.x]];
   if (d.M != M) return;
   const int N = d.N, n = d.n;
   const long long o = d.bhat2;
   const double2 *W = twiddle + d.tw;
+  for (int j = threadIdx.x; j < N; j += M / 16) chirp[d.chirp + j] = pb_chirp(W, j, n);
   for (int j = threadIdx.x; j < M; j += M / 16) {
     const int jj = j < N ? j : (j > M - N ? M - j : -1);
     smem[pw_pad(j)] = jj >= 0 ? cconj(pb_chirp(W, jj, n)) : make_double2(0.0, 0.0);
@@ -1170,9 +1171,9 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
                        const double *__restrict__ weight, const int *__restrict__ fftidx,
                        const FftDesc *__restrict__ fdesc, const double2 *__restrict__ twiddle,
                        const double2 *__restrict__ wpow2, int P,
-                       const double2 *__restrict__ bhat, const double2 *__restrict__ phase,
-                       int ncm, int mmax, int flags, T *const *__restrict__ maps,
-                       long long map_lo) {
+                       const double2 *__restrict__ bhat, const double2 *__restrict__ chirp,
+                       const double2 *__restrict__ phase, int ncm, int mmax, int flags,
+                       T *const *__restrict__ maps, long long map_lo) {
   constexpr int NT = M / 16;
   extern __shared__ double2 smem[];
   double2 *buf = smem;
@@ -1186,6 +1187,7 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   const FftDesc &fd = fdesc[fftidx[ring]];
   const double2 *W = twiddle + fd.tw;     // exp(-2 pi i e/n)
   const double2 *bh = bhat + fd.bhat2;
+  const double2 *cz = chirp + fd.chirp;   // c_j, j < N
   const int ms = mmax + 1;
   const int mm = min(mmax, mlim[p]);
   const bool add = (flags & (SHARP_ADD | SHARP_SUBTRACT)) != 0;
@@ -1226,7 +1228,7 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
       const double2 sm = cadd(ck, cn), df = csub(ck, cn);
       const double2 w = __ldg(W + k);
       const double2 iw = make_double2(w.y, w.x);   // i * conj(w)
-      v[i] = cmul(cconj(cadd(sm, cmul(iw, df))), pb_chirp(W, k, n));
+      v[i] = cmul(cconj(cadd(sm, cmul(iw, df))), __ldg(cz + k));
     }
   }
   __syncthreads();
@@ -1237,7 +1239,7 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   T *map = maps[c] + (ofs[ring] - map_lo);
   const long long st = stride[ring];
   for (int j = threadIdx.x; j < N; j += NT) {
-    const double2 z = cmul(buf[pw_pad(j)], pb_chirp(W, j, n));
+    const double2 z = cmul(buf[pw_pad(j)], __ldg(cz + j));
     store_px(map + (2 * j) * st, z.x, add);
     store_px(map + (2 * j + 1) * st, -z.y, add);
   }
@@ -1252,9 +1254,9 @@ ring2phase_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
                        const double *__restrict__ weight, const int *__restrict__ fftidx,
                        const FftDesc *__restrict__ fdesc, const double2 *__restrict__ twiddle,
                        const double2 *__restrict__ wpow2, int P,
-                       const double2 *__restrict__ bhat, double2 *__restrict__ phase, int ncm,
-                       int mmax, int flags, const T *const *__restrict__ maps,
-                       long long map_lo) {
+                       const double2 *__restrict__ bhat, const double2 *__restrict__ chirp,
+                       double2 *__restrict__ phase, int ncm, int mmax, int flags,
+                       const T *const *__restrict__ maps, long long map_lo) {
   constexpr int NT = M / 16;
   extern __shared__ double2 smem[];
   double2 *buf = smem;
@@ -1268,6 +1270,7 @@ ring2phase_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   const FftDesc &fd = fdesc[fftidx[ring]];
   const double2 *W = twiddle + fd.tw;
   const double2 *bh = bhat + fd.bhat2;
+  const double2 *cz = chirp + fd.chirp;   // c_j, j < N
   const int ms = mmax + 1;
   const int mm = min(mmax, mlim[p]);
   const double wgt = ((flags & SHARP_USE_WEIGHTS) ? weight[ring] : 1.0) *
@@ -1286,7 +1289,7 @@ ring2phase_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
     v[i] = make_double2(0.0, 0.0);
     if (i < 8 && j < N)
       v[i] = cmul(make_double2(double(map[(2 * j) * st]), double(map[(2 * j + 1) * st])),
-                  pb_chirp(W, j, n));
+                  __ldg(cz + j));
   }
   pw_pass16_regs<M, false>(v, buf, M, wpow2, P);
   __syncthreads();
@@ -1302,8 +1305,8 @@ ring2phase_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   };
   for (int k = threadIdx.x; 2 * k <= N; k += NT) {
     const int kk = N - k;
-    const double2 zk = cmul(buf[pw_pad(k)], pb_chirp(W, k, n));
-    const double2 zn = (k == 0) ? zk : cmul(buf[pw_pad(kk)], pb_chirp(W, kk, n));
+    const double2 zk = cmul(buf[pw_pad(k)], __ldg(cz + k));
+    const double2 zn = (k == 0) ? zk : cmul(buf[pw_pad(kk)], __ldg(cz + kk));
     double2 xk = xout(zk, zn, k), xn = xout(zn, zk, kk);
     if (k == 0) { xk.y = 0.0; xn.y = 0.0; }   // DC and Nyquist are real
     buf[pw_pad(k)] = xk;
@@ -1554,7 +1557,7 @@ void launch_bluestein_pw_setup(const GeomPlan &gp, const int *d_blue2_idx, int n
     SHT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)));
     kernel<<<nblue2, M / 16, smem, st>>>(gp.fdesc, d_blue2_idx, gp.twiddle, gp.wpow2, gp.P,
-                                         gp.bhat);
+                                         gp.bhat, gp.chirp);
     SHT_CUDA(cudaGetLastError());
   };
   if (gp.P >= 1024) one(bluestein_pw_setup_kernel<1024>, 1024);
@@ -1724,8 +1727,8 @@ void phase2ring_blue(const JobDesc &job, const GeomPlan &gp, int cls, long long 
   SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   k<<<dim3(2 * gp.pb_count[cls], nmapptr), M / 16, smem, st>>>(
       gp.pb_pairs + gp.pb_start[cls], gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
-      gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm, job.mmax, job.flags,
-      reinterpret_cast<T *const *>(maps_dev), map_lo);
+      gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, gp.chirp, phase, ncm, job.mmax,
+      job.flags, reinterpret_cast<T *const *>(maps_dev), map_lo);
   SHT_CUDA(cudaGetLastError());
 }
 
@@ -1738,8 +1741,8 @@ void ring2phase_blue(const JobDesc &job, const GeomPlan &gp, int cls, long long 
   SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   k<<<dim3(2 * gp.pb_count[cls], nmapptr), M / 16, smem, st>>>(
       gp.pb_pairs + gp.pb_start[cls], gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
-      gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, phase, ncm, job.mmax, job.flags,
-      reinterpret_cast<const T *const *>(maps_dev), map_lo);
+      gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, gp.chirp, phase, ncm, job.mmax,
+      job.flags, reinterpret_cast<const T *const *>(maps_dev), map_lo);
   SHT_CUDA(cudaGetLastError());
 }
 
