@@ -569,3 +569,15 @@ def test_register_bluestein_rings_match_reference(ref, spin, flags):
     ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, flags)
     for x, y in zip(b1, b2):
         assert rel_l2(x, y) < tol
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_healpix_nside512_lmax1024_both_directions(ref, spin):
+    # Nside 512: the equatorial rings (2048 pixels) take the power-of-two
+    # register FFT of length 1024 (the shortest), the polar rings the
+    # register Bluestein lengths 1024 and 2048 and the size classes; both
+    # directions against the reference at 1e-12
+    for jtype in (1, 0):
+        o1, o2 = run_pair(ref, ("healpix", 512), 1024, 1024, spin, jtype, seed=11 + spin)
+        for x, y in zip(o1, o2):
+            assert rel_l2(x, y) < TOL, (spin, jtype)
