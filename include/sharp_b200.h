@@ -141,6 +141,14 @@ typedef struct {
 int sharp_b200_execute_batch (const sharp_b200_job *jobs, int njobs,
   int device_ptrs, void *stream, unsigned long long *opcnt);
 
+/* How sharp_b200_execute_batch would merge `jobs` (same arguments): returns
+   the number of merged groups and, if group_of_job is non-NULL, each job's
+   group index (groups numbered in order of first appearance), or -1 after
+   an argument error in non-abort mode.  Host work only: nothing runs on the
+   GPU and no array is read. */
+int sharp_b200_batch_groups (const sharp_b200_job *jobs, int njobs,
+  int device_ptrs, int *group_of_job);
+
 /* Spin-0 alm2map without any device allocation.  No counterpart in the
    reference: it serves callers that cannot call cudaMalloc when they need a
    transform (GPU memory owned by another allocator such as a framework's

@@ -1138,15 +1138,18 @@ std::pair<uintptr_t, uintptr_t> host_span(const void *base, const sharp_b200_job
 // execute_impl.  With host arrays a job may read what an earlier job writes:
 // such batches merge only consecutive jobs, so that no job moves ahead of
 // one it depends on.  Returns the number of merged jobs.
-int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
-                       cudaStream_t stream, unsigned long long *opcnt) {
+struct BatchGroup {
+  const sharp_b200_job *first;
+  std::vector<void *> alm, map;
+  int ntrans = 0;
+};
+
+// The merged groups of a batch, in order; group_of (if given) receives each
+// job's group index.  Host work only.
+std::vector<BatchGroup> group_batch(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
+                                    std::vector<int> *group_of) {
   SHT_REQUIRE(njobs >= 0 && (jobs != nullptr || njobs == 0), "bad job list");
-  struct Group {
-    const sharp_b200_job *first;
-    std::vector<void *> alm, map;
-    int ntrans = 0;
-  };
-  std::vector<Group> groups;
+  std::vector<BatchGroup> groups;
   // pointers per transform before the type remap (sharp.c:855-856)
   auto counts = [](const sharp_b200_job &j, int &na, int &nm) {
     const bool deriv = j.type == SHARP_ALM2MAP_DERIV1;
@@ -1194,6 +1197,7 @@ int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
       if (dependent) break;
     }
   }
+  if (group_of) group_of->assign(njobs, -1);
   for (int i = 0; i < njobs; ++i) {
     const sharp_b200_job &j = jobs[i];
     int na, nm;
@@ -1201,28 +1205,36 @@ int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
     // independent jobs: any earlier group; a host batch with dependences:
     // the last group only, so that merging never moves a job ahead of one
     // it depends on
-    Group *g = nullptr;
+    int gi = -1;
     for (size_t k = dependent ? (groups.empty() ? 0 : groups.size() - 1) : 0;
          k < groups.size(); ++k) {
-      Group &c = groups[k];
+      const BatchGroup &c = groups[k];
       const sharp_b200_job &f = *c.first;
       if (f.type == j.type && f.spin == j.spin && f.flags == j.flags &&
           f.geom_info == j.geom_info && f.alm_info == j.alm_info &&
           c.ntrans + j.ntrans <= kMaxTrans) {
-        g = &c;
+        gi = int(k);
         break;
       }
     }
-    if (!g) {
-      groups.push_back(Group{&j, {}, {}, 0});
-      g = &groups.back();
+    if (gi < 0) {
+      groups.push_back(BatchGroup{&j, {}, {}, 0});
+      gi = int(groups.size()) - 1;
     }
+    BatchGroup *g = &groups[gi];
     void *const *pa = static_cast<void *const *>(j.alm);
     void *const *pm = static_cast<void *const *>(j.map);
     g->alm.insert(g->alm.end(), pa, pa + size_t(j.ntrans) * na);
     g->map.insert(g->map.end(), pm, pm + size_t(j.ntrans) * nm);
     g->ntrans += j.ntrans;
+    if (group_of) (*group_of)[i] = gi;
   }
+  return groups;
+}
+
+int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
+                       cudaStream_t stream, unsigned long long *opcnt) {
+  std::vector<BatchGroup> groups = group_batch(jobs, njobs, device_ptrs, nullptr);
   unsigned long long tot = 0;
   // host arrays: every merged group through one pipelined sequence of pieces
   // (one fill and one drain for the batch) where each group allows it
@@ -1262,7 +1274,7 @@ int execute_batch_impl(const sharp_b200_job *jobs, int njobs, bool device_ptrs,
       for (int gi : order) {
         const int lane = int(std::min_element(load.begin(), load.end()) - load.begin());
         load[lane] += cost(gi);
-        Group &g = groups[gi];
+        BatchGroup &g = groups[gi];
         unsigned long long oc = 0;
         execute_impl(g.first->type, g.first->spin, g.alm.data(), g.map.data(),
                      g.first->geom_info, g.first->alm_info, g.ntrans, g.first->flags, true,
@@ -1337,6 +1349,17 @@ void sharp_b200_execute_device(sharp_jobtype type, int spin, void *alm, void *ma
     sht::execute_impl(type, spin, alm, map, geom_info, alm_info, ntrans, flags, true,
                       static_cast<cudaStream_t>(stream), time, opcnt);
   });
+}
+
+int sharp_b200_batch_groups(const sharp_b200_job *jobs, int njobs, int device_ptrs,
+                            int *group_of_job) {
+  int n = -1;
+  sht::guarded([&] {
+    std::vector<int> of;
+    n = int(sht::group_batch(jobs, njobs, device_ptrs != 0, &of).size());
+    if (group_of_job) std::copy(of.begin(), of.end(), group_of_job);
+  });
+  return n;
 }
 
 int sharp_b200_execute_batch(const sharp_b200_job *jobs, int njobs, int device_ptrs,

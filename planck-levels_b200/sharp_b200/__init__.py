@@ -340,6 +340,36 @@ _lib.sharp_b200_execute_batch.argtypes = [C.POINTER(sharp_b200_job), C.c_int, C.
 _lib.sharp_b200_execute_batch.restype = C.c_int
 
 
+def _job_array(jobs, device):
+    """sharp_b200_job array of the job tuples (and the pointer arrays it uses)."""
+    keep = []
+    arr = (sharp_b200_job * max(len(jobs), 1))()
+    for i, (jt, spin, alm, maps, geom, ainfo, nt, fl) in enumerate(jobs):
+        ptr = (lambda a: a.data_ptr()) if device else (lambda a: a.ctypes.data)
+        aptr = (C.c_void_p * len(alm))(*[ptr(a) for a in alm])
+        mptr = (C.c_void_p * len(maps))(*[ptr(m) for m in maps])
+        keep += [aptr, mptr]
+        arr[i] = sharp_b200_job(jt, spin, C.cast(aptr, C.c_void_p), C.cast(mptr, C.c_void_p),
+                                geom.ptr, ainfo.ptr, nt, fl)
+    return arr, keep
+
+
+_lib.sharp_b200_batch_groups.argtypes = [C.POINTER(sharp_b200_job), C.c_int, C.c_int,
+                                         C.POINTER(C.c_int)]
+_lib.sharp_b200_batch_groups.restype = C.c_int
+
+
+def batch_groups(jobs, device: bool = False):
+    """sharp_b200_batch_groups: how ``execute_batch`` would merge ``jobs``
+    (same tuples); returns the group index of every job.  Host work only."""
+    arr, keep = _job_array(jobs, device)
+    of = (C.c_int * max(len(jobs), 1))()
+    n = _lib.sharp_b200_batch_groups(arr, len(jobs), 1 if device else 0, of)
+    _check()
+    assert n >= 0
+    return [of[i] for i in range(len(jobs))]
+
+
 def execute_batch(jobs, device: bool = False, stream=None):
     """sharp_b200_execute_batch: ``jobs`` is a list of tuples
     (jtype, spin, alm, maps, geom, ainfo, ntrans, flags) with alm/maps lists
@@ -350,15 +380,7 @@ def execute_batch(jobs, device: bool = False, stream=None):
     halves of a round trip; only consecutive jobs merge); with device arrays
     the jobs must be independent.  Returns (number of merged jobs, operation
     count)."""
-    keep = []
-    arr = (sharp_b200_job * max(len(jobs), 1))()
-    for i, (jt, spin, alm, maps, geom, ainfo, nt, fl) in enumerate(jobs):
-        ptr = (lambda a: a.data_ptr()) if device else (lambda a: a.ctypes.data)
-        aptr = (C.c_void_p * len(alm))(*[ptr(a) for a in alm])
-        mptr = (C.c_void_p * len(maps))(*[ptr(m) for m in maps])
-        keep += [aptr, mptr]
-        arr[i] = sharp_b200_job(jt, spin, C.cast(aptr, C.c_void_p), C.cast(mptr, C.c_void_p),
-                                geom.ptr, ainfo.ptr, nt, fl)
+    arr, keep = _job_array(jobs, device)
     st = None
     if device:
         import torch
