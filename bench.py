@@ -15,8 +15,11 @@ Two forms are measured in the same run:
   * fp64: the plain FP64 drop-in, one set per step (ntrans = 1).
 One step = T+QU alm2map followed by T+QU map2alm for each set of the step.
 ``value`` has the inputs resident in HBM; ``e2e`` is the same metric through
-the C ABI (sharp_execute) with pinned host buffers, so every step includes
-the host<->device copies.  N>1 runs independent replicas (the transform does
+the C ABI with pinned host buffers, so every step includes the host<->device
+copies: one sharp_b200_execute_batch call per step holding the round trip
+(T and QU alm2map, then T and QU map2alm of the maps just written to host
+memory), with the figures for one batch call per direction and for four
+sharp_execute calls beside it.  N>1 runs independent replicas (the transform does
 not shard across GPUs in this workload).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
