@@ -1162,9 +1162,15 @@ bluestein_pw_setup_kernel(const FftDesc *__restrict__ fdesc, const int *__restri
     bhat[o + j] = cscale(smem[pw_pad(j)], 1.0 / M);
 }
 
+// CTAs per SM the register Bluestein kernels are compiled for (at most 128
+// registers: two CTAs of 256 threads at M = 4096 instead of one at ~150)
+__host__ __device__ constexpr int blue_min_blocks(int M) {
+  return M == 4096 ? 2 : M == 2048 ? 4 : M == 1024 ? 8 : 1;
+}
+
 // phase -> ring.  Grid: (2 * pairs of this length, components).
 template <typename T, int M>
-__global__ void __launch_bounds__(M / 16)
+__global__ void __launch_bounds__(M / 16, blue_min_blocks(M))
 phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
                        const int *__restrict__ nph, const long long *__restrict__ ofs,
                        const int *__restrict__ stride, const double *__restrict__ phi0,
@@ -1247,7 +1253,7 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
 
 // ring -> phase
 template <typename T, int M>
-__global__ void __launch_bounds__(M / 16)
+__global__ void __launch_bounds__(M / 16, blue_min_blocks(M))
 ring2phase_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ mlim,
                        const int *__restrict__ nph, const long long *__restrict__ ofs,
                        const int *__restrict__ stride, const double *__restrict__ phi0,
