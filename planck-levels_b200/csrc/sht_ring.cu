@@ -1179,12 +1179,16 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
                        const double2 *__restrict__ wpow2, int P,
                        const double2 *__restrict__ bhat, const double2 *__restrict__ chirp,
                        const double2 *__restrict__ phase, int ncm, int mmax, int flags,
-                       T *const *__restrict__ maps, long long map_lo) {
+                       T *const *__restrict__ maps, long long map_lo, int stage_row) {
   constexpr int NT = M / 16;
   extern __shared__ double2 smem[];
+  __shared__ uint64_t row_full;
   double2 *buf = smem;
   double2 *slo = smem + pw_entries(M);
   double2 *shi = slo + kShiftLo;
+  // stage_row: the phase row (mm + 1 <= mmax + 1 entries) is copied into
+  // shared memory behind the phi0 slices, so the alias fold reads it there
+  double2 *srow = shi + (mmax / kShiftLo + 2);
   const int p = pairs[blockIdx.x >> 1], h = blockIdx.x & 1, c = blockIdx.y;
   const int ring = 2 * p + h;
   const int n = nph[ring];
@@ -1203,10 +1207,29 @@ phase2ring_blue_kernel(const int *__restrict__ pairs, const int *__restrict__ ml
   const double ph = phi0[ring];
   const bool rot = fabs(ph) >= 1e-14;
   const double2 *src = phase + ((long long)(p * ncm + c) * 2 + h) * ms;
+  if (stage_row) {
+    if (threadIdx.x == 0) {
+      mbar_init(&row_full, 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_arrive_tx(&row_full, uint32_t(16 * (mm + 1)));
+      bulk_g2s(srow, src, uint32_t(16 * (mm + 1)), &row_full);
+    }
+  }
   if (rot) build_shift(slo, shi, mm, ph);
+  if (stage_row) {
+    // a copy that did not complete within the bounded wait is redone by
+    // the threads (the same values)
+    if (__syncthreads_or(!mbar_wait(&row_full, 0))) {
+      for (int m = threadIdx.x; m <= mm; m += NT) srow[m] = src[m];
+    }
+  }
   __syncthreads();
+  const double2 *row = stage_row ? srow : src;
   auto tm = [&](int m) {
-    double2 t = cscale(src[m], wgt);
+    double2 t = cscale(row[m], wgt);
     if (rot) t = cmul(t, shift_of(slo, shi, m));
     return t;
   };
@@ -1729,12 +1752,17 @@ void phase2ring_blue(const JobDesc &job, const GeomPlan &gp, int cls, long long 
                      const double2 *phase, int ncm, void *const *maps_dev, int nmapptr,
                      cudaStream_t st) {
   auto k = phase2ring_blue_kernel<T, M>;
-  const size_t smem = pow2_smem(M, job.mmax);
+  // the phase row is staged in shared memory where that keeps the CTAs per
+  // SM (M = 8192: one CTA per SM either way) and fits
+  const size_t base = pow2_smem(M, job.mmax);
+  const size_t with_row = base + sizeof(double2) * (job.mmax + 1);
+  const int stage_row = (M == 8192 && with_row + 1024 <= 227 * 1024) ? 1 : 0;
+  const size_t smem = stage_row ? with_row : base;
   SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   k<<<dim3(2 * gp.pb_count[cls], nmapptr), M / 16, smem, st>>>(
       gp.pb_pairs + gp.pb_start[cls], gp.mlim, gp.nph, gp.ofs, gp.stride, gp.phi0, gp.weight,
       gp.fft, gp.fdesc, gp.twiddle, gp.wpow2, gp.P, gp.bhat, gp.chirp, phase, ncm, job.mmax,
-      job.flags, reinterpret_cast<T *const *>(maps_dev), map_lo);
+      job.flags, reinterpret_cast<T *const *>(maps_dev), map_lo, stage_row);
   SHT_CUDA(cudaGetLastError());
 }
 
