@@ -597,7 +597,8 @@ def run_ours(args, world, rank, local, clk, np, torch, sb):
                                    f"lmax=mmax={lmax}, spin 0+2, {form}",
                        "nside": nside, "lmax": lmax, "form": args.form, "batch": B,
                        "alm": "a_lm ~ C_l = (l+1)^-2 exp(-l(l+1) sigma^2), sigma 5', E 0.1, B 0.01",
-                       "l2": "inputs larger than L2 (each map 403 MB, each a_lm 134 MB)",
+                       "l2": f"inputs larger than L2 (each map {npix * 8 / 1e6:.0f} MB, "
+                             f"each a_lm {nalm * 16 / 1e6:.0f} MB)",
                        "parallelism": f"replicas x{world}"},
             "rel_err_vs_fp64": err,
             "fp64_dropin": {"value": world / fp64_s, "unit": UNIT, "ms_per_step": fp64_s * 1e3,
