@@ -13,7 +13,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <cstdio>
 #include <functional>
+#include <tuple>
 #include <map>
 #include <set>
 #include <memory>
@@ -637,6 +639,86 @@ double wall_now() {
 // ---------------------------------------------------------------------------
 // the job
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Pass-width tuner, the counterpart of the reference's nv oracle
+// (libsharp/sharp.c:890-965, which times its SIMD vector counts on first
+// use): the FP64 Legendre kernels take 1, 2 or 4 transforms per pass (spin s
+// and deriv1: 1 or 2); wider passes share one recurrence, narrower ones keep
+// more CTAs per SM, and which wins depends on the geometry, lmax and spin.
+// The first job of a shape with several transforms times each width once on
+// its own buffers (after one untimed run of it; one host synchronisation per
+// width) and the fastest is kept for the process, the default width unless
+// another is more than 3% faster.  Jobs whose flags carry a vector-count hint (the low bits,
+// SHARP_NVMAX, as the reference's nv), jobs on a stream that is being
+// captured, and all jobs when SHARP_B200_TUNE=0 keep the default widths;
+// SHARP_B200_TUNE_LOG prints each decision with its timings to stderr.
+// ---------------------------------------------------------------------------
+struct TuneKey {
+  uint64_t geom;
+  int lmax, mmax, spin, type, ntrans, pass;   // pass: 0 synthesis, 1 analysis
+  bool operator<(const TuneKey &o) const {
+    return std::tie(geom, lmax, mmax, spin, type, ntrans, pass) <
+           std::tie(o.geom, o.lmax, o.mmax, o.spin, o.type, o.ntrans, o.pass);
+  }
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, int> g_tuned;
+
+bool tuner_on(int flags, cudaStream_t st) {
+  static const bool env_on = [] {
+    const char *e = getenv("SHARP_B200_TUNE");
+    return !(e && e[0] == '0');
+  }();
+  if (!env_on || (flags & SHARP_NVMAX) != 0) return false;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone;
+}
+
+// run(w) enqueues every pass of the job with width w on st; reset() undoes
+// what the timing runs accumulated.  Returns the width to use.
+int tuned_width(const TuneKey &key, int wmax, int wdefault, const std::function<void(int)> &run,
+                const std::function<void()> &reset, cudaStream_t st) {
+  std::lock_guard<std::mutex> lk(g_tune_mutex);
+  auto it = g_tuned.find(key);
+  if (it != g_tuned.end()) return it->second;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SHT_CUDA(cudaEventCreate(&e0));
+  SHT_CUDA(cudaEventCreate(&e1));
+  std::vector<std::pair<int, float>> times;
+  for (int w = 1; w <= wmax; w *= 2) {
+    run(w);   // untimed: first launch of the width's kernels, first touch of the buffers
+    SHT_CUDA(cudaEventRecord(e0, st));
+    run(w);
+    SHT_CUDA(cudaEventRecord(e1, st));
+    SHT_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SHT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    times.push_back({w, ms});
+  }
+  SHT_CUDA(cudaEventDestroy(e0));
+  SHT_CUDA(cudaEventDestroy(e1));
+  reset();
+  float tdef = 0.f;
+  for (auto &t : times)
+    if (t.first == wdefault) tdef = t.second;
+  int best = wdefault;
+  float tbest = tdef;
+  for (auto &t : times)
+    if (t.second < tbest && t.second < 0.97f * tdef) {
+      best = t.first;
+      tbest = t.second;
+    }
+  g_tuned[key] = best;
+  static const bool log = getenv("SHARP_B200_TUNE_LOG") != nullptr;
+  if (log) {
+    std::fprintf(stderr, "sharp_b200 tuner: %s spin %d lmax %d ntrans %d:",
+                 key.pass ? "analysis" : "synthesis", key.spin, key.lmax, key.ntrans);
+    for (auto &t : times) std::fprintf(stderr, " width %d %.3f ms", t.first, t.second);
+    std::fprintf(stderr, " -> %d\n", best);
+  }
+  return best;
+}
+
 void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
                   const sharp_geom_info *ginfo, const sharp_alm_info *ainfo, int ntrans,
                   int flags, bool device_ptrs, cudaStream_t user_stream, double *time,
@@ -790,12 +872,20 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
       tc_error_word(&d_err);
       launch_mixed_synth(job, *gp, *cp, d_A.as<double2>(), ncA, phase, ncm, d_err, st);
     } else {
-      for (int t0 = 0; t0 < ntrans;) {
-        const int nt = group(ntrans - t0, ntmax_synth);
-        launch_legendre_synth(job, *gp, *cp, d_A.as<double2>(), ncA, t0 * job.nalm, nt, phase,
-                              ncm, t0 * job.nmaps, st);
-        t0 += nt;
-      }
+      auto passes = [&](int width) {
+        for (int t0 = 0; t0 < ntrans;) {
+          const int nt = group(ntrans - t0, width);
+          launch_legendre_synth(job, *gp, *cp, d_A.as<double2>(), ncA, t0 * job.nalm, nt,
+                                phase, ncm, t0 * job.nmaps, st);
+          t0 += nt;
+        }
+      };
+      int width = ntmax_synth;
+      if (ntrans >= 2 && tuner_on(flags, st))
+        // synthesis passes overwrite the phase rows, so the timing runs leave nothing behind
+        width = tuned_width(TuneKey{gp->hash, job.lmax, mmax, spin, type, ntrans, 0},
+                            ntmax_synth, ntmax_synth, passes, [] {}, st);
+      passes(width);
     }
     if (no_fft)
       launch_phase2ring_direct(job, *gp, map_lo, phase, ncm,
@@ -822,12 +912,24 @@ void execute_impl(sharp_jobtype type_in, int spin, void *alm, void *map,
       tc_error_word(&d_err);
       launch_mixed_anal(job, *gp, *cp, phase, ncm, d_Aout.as<double2>(), ncA, d_err, st);
     } else {
-      for (int t0 = 0; t0 < ntrans;) {
-        const int nt = group(ntrans - t0, ntmax_anal);
-        launch_legendre_anal(job, *gp, *cp, phase, ncm, t0 * job.nmaps, nt,
-                             d_Aout.as<double>(), ncA, t0 * job.nalm, st);
-        t0 += nt;
+      auto passes = [&](int width) {
+        for (int t0 = 0; t0 < ntrans;) {
+          const int nt = group(ntrans - t0, width);
+          launch_legendre_anal(job, *gp, *cp, phase, ncm, t0 * job.nmaps, nt,
+                               d_Aout.as<double>(), ncA, t0 * job.nalm, st);
+          t0 += nt;
+        }
+      };
+      int width = ntmax_anal;
+      if (ntrans >= 2 && tuner_on(flags, st)) {
+        // analysis passes accumulate into Aout: cleared again after the timing runs
+        auto clear = [&] {
+          SHT_CUDA(cudaMemsetAsync(d_Aout.p, 0, sizeof(double2) * size_t(cp->total) * ncA, st));
+        };
+        width = tuned_width(TuneKey{gp->hash, job.lmax, mmax, spin, type, ntrans, 1},
+                            spin == 0 ? 4 : 2, ntmax_anal, passes, clear, st);
       }
+      passes(width);
     }
     launch_scatter_alm(job, *ap, alm_lo, *cp, d_norm.as<double>(), d_Aout.as<double>(), ncA,
                        reinterpret_cast<void *const *>(d_almptr.p), nalmptr, st);
