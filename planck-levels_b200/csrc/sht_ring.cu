@@ -7,7 +7,18 @@
 // and the SHARP_NO_FFT path); FFT conventions of libfftpack/ls_fft.c:130-212
 // (unnormalised backward transform, FFTPACK half-complex order).
 //
-// One CTA owns one (ring pair, component) and runs both hemispheres.  The FFT
+// Three kernel families, chosen per ring pair when the geometry plan is built:
+//  * power-of-two rings (2N pixels, N = 1024 .. 8192, no alias folding): one
+//    CTA per ring and component, radix-16 passes in registers
+//    (phase2ring_pow2_kernel / ring2phase_pow2_kernel);
+//  * long even rings that need a Bluestein convolution of length M = 1024 ..
+//    8192 (the polar HEALPix rings): the same register passes around the
+//    chirp product (phase2ring_blue_kernel / ring2phase_blue_kernel);
+//  * all other rings, in size classes (phase2ring_kernel / ring2phase_kernel),
+//    described here.
+//
+// Size classes: one CTA owns one (ring pair, component) and runs both
+// hemispheres.  The FFT
 // is a Stockham auto-sort mixed-radix transform in shared memory: even ring
 // lengths n use a complex FFT of length n/2 on packed (x_2j + i x_2j+1) data;
 // odd lengths a complex FFT of length n.  Radix-2/3/4/5/8 stages and a generic
