@@ -448,7 +448,10 @@ def phase2ring(ring: Ring, phase, mmax, flags):
     spec[0] += tmp[0].real
     if mmax >= 1:
         mm = m[1:]; t = tmp[1:]
-        i1 = mm % nph
+        # the reference's running index starts at 1 for m = 1 and wraps only
+        # after it (sharp.c:282, :297): for a one-pixel ring the direct term
+        # of m = 1 falls outside the bins and is dropped
+        i1 = np.where(mm == 1, 1, mm % nph)
         ok1 = i1 < (nph + 2) // 2
         np.add.at(spec, i1[ok1], t[ok1])
         i2 = (nph - mm % nph) % nph

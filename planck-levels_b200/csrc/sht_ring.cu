@@ -535,10 +535,14 @@ __global__ void __launch_bounds__(1024) phase2ring_kernel(const int *__restrict_
     if (rot) build_shift(slo, shi, mm, ph);
     load_twshared(twlo, twhi, twiddle + d.tw, n);
     __syncthreads();
-    // fold phase_m * wgt * e^{i m phi0} into bins 0..half (sharp.c:265-300)
+    // fold phase_m * wgt * e^{i m phi0} into bins 0..half (sharp.c:265-300);
+    // as there, the direct term of m = 1 of a one-pixel ring is not added
+    // (the reference's running bin index starts at 1 and wraps only after
+    // its first use, sharp.c:282, :297)
     for (int k = threadIdx.x; k <= half; k += blockDim.x) {
       double2 acc = make_double2(0.0, 0.0);
       for (int m = k; m <= mm; m += n) {
+        if (n == 1 && m == 1) continue;
         double2 t = cscale(src[m], wgt);
         if (rot) t = cmul(t, shift_of(slo, shi, m));
         acc = cadd(acc, t);

@@ -581,3 +581,40 @@ def test_healpix_nside512_lmax1024_both_directions(ref, spin):
         o1, o2 = run_pair(ref, ("healpix", 512), 1024, 1024, spin, jtype, seed=11 + spin)
         for x, y in zip(o1, o2):
             assert rel_l2(x, y) < TOL, (spin, jtype)
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_every_ring_length_1_to_4096_matches_reference(ref, spin):
+    # the counterpart of the reference's ffttest (every length 1..4096): one
+    # ring of each length, unpaired, at distinct colatitudes, phi0 shifts and
+    # weights; lmax 64, so the short rings fold the phases and the long ones
+    # take every FFT path (size classes with all radix mixes and Bluestein,
+    # power-of-two rings, register Bluestein); both directions at 1e-12
+    nph = np.arange(1, 4097, dtype=np.int32)
+    nr = len(nph)
+    theta = np.linspace(0.02, np.pi / 2 - 0.02, nr)
+    ofs = np.concatenate([[0], np.cumsum(nph)[:-1]])
+    st = np.ones(nr, np.int32)
+    phi0 = np.linspace(0.0, 1.0, nr)
+    w = np.linspace(0.5, 1.5, nr) * 4 * np.pi / nph.sum()
+    g1 = sb.Geometry.general(nph, ofs, st, phi0, theta, w)
+    g2 = ref.general(nph, ofs, st, phi0, theta, w)
+    lmax = 64
+    a1, a2 = sb.AlmInfo.triangular(lmax), ref.triangular(lmax, lmax)
+    npix = int(nph.sum())
+    na = _nalm(1, spin)
+    alms = [uniform_alm(lmax, seed=60 + i, spin=spin) for i in range(na)]
+    m1 = [np.zeros(npix) for _ in range(na)]
+    m2 = [np.zeros(npix) for _ in range(na)]
+    sb.execute(1, spin, [x.copy() for x in alms], m1, g1, a1, 1, DP)
+    ref.execute(1, spin, [x.copy() for x in alms], m2, g2, a2, 1, DP)
+    for x, y in zip(m1, m2):
+        assert rel_l2(x, y) < TOL
+    rng = np.random.default_rng(29 + spin)
+    maps = [rng.standard_normal(npix) for _ in range(na)]
+    b1 = [np.zeros(sb.nalm_triangular(lmax), np.complex128) for _ in range(na)]
+    b2 = [x.copy() for x in b1]
+    sb.execute(0, spin, b1, [x.copy() for x in maps], g1, a1, 1, DP)
+    ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, DP)
+    for x, y in zip(b1, b2):
+        assert rel_l2(x, y) < TOL

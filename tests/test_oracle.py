@@ -165,3 +165,41 @@ def test_oracle_prime_ring_lengths_against_reference_library():
         so.execute(0, spin, b_or, [m.copy() for m in maps], geo, ai, 1, 16)
         for i in range(na):
             assert rel_l2(b_or[i], b_ref[i]) < 1e-12
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_oracle_every_short_ring_length_against_reference_library(spin):
+    # rings of every length 1..96 (alias folding for all but the longest at
+    # lmax 64, including the one-pixel ring whose m = 1 direct term the
+    # reference's fold drops), phi0 shifts and weights, both directions
+    ref = pytest.importorskip("ref")
+    if not ref.available():
+        pytest.skip("reference library not built (make -C oracle)")
+    nph = np.arange(1, 97, dtype=np.int32)
+    nr = len(nph)
+    theta = np.linspace(0.02, np.pi / 2 - 0.02, nr)
+    ofs = np.concatenate([[0], np.cumsum(nph)[:-1]])
+    st = np.ones(nr, np.int32)
+    phi0 = np.linspace(0.0, 1.0, nr)
+    w = np.linspace(0.5, 1.5, nr)
+    g2 = ref.general(nph, ofs, st, phi0, theta, w)
+    go = so.make_geom_info(nph, ofs, st, phi0, theta, w)
+    lmax = 64
+    a2, ao = ref.triangular(lmax, lmax), so.triangular_alm_info(lmax, lmax)
+    na = 1 if spin == 0 else 2
+    alms = [uniform_alm(lmax, seed=60 + i, spin=spin) for i in range(na)]
+    npix = int(nph.sum())
+    m_ref = [np.zeros(npix) for _ in range(na)]
+    m_or = [np.zeros(npix) for _ in range(na)]
+    ref.execute(1, spin, [x.copy() for x in alms], m_ref, g2, a2, 1, so.SHARP_DP)
+    so.execute(so.SHARP_ALM2MAP, spin, [x.copy() for x in alms], m_or, go, ao, 1, so.SHARP_DP)
+    for x, y in zip(m_or, m_ref):
+        assert rel_l2(x, y) < 1e-13
+    rng = np.random.default_rng(5)
+    maps = [rng.standard_normal(npix) for _ in range(na)]
+    b_ref = [np.zeros_like(alms[0]) for _ in range(na)]
+    b_or = [np.zeros_like(alms[0]) for _ in range(na)]
+    ref.execute(0, spin, b_ref, [x.copy() for x in maps], g2, a2, 1, so.SHARP_DP)
+    so.execute(so.SHARP_MAP2ALM, spin, b_or, [x.copy() for x in maps], go, ao, 1, so.SHARP_DP)
+    for x, y in zip(b_or, b_ref):
+        assert rel_l2(x, y) < 1e-13
