@@ -618,3 +618,41 @@ def test_every_ring_length_1_to_4096_matches_reference(ref, spin):
     ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, DP)
     for x, y in zip(b1, b2):
         assert rel_l2(x, y) < TOL
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_ring_lengths_with_folding_at_high_lmax(ref, spin):
+    # lmax 2100 folds the phases of every ring up to 4200 pixels: lengths
+    # 1..4096 in steps of 7 plus the power-of-two and neighbouring lengths
+    # (the register FFT classes then take folded rings: 4096 pixels goes to
+    # the register Bluestein convolution of length 4096), unpaired rings,
+    # phi0 shifts and weights; both directions at 1e-12
+    nph = np.unique(np.concatenate([np.arange(1, 4097, 7), [2047, 2048, 2049, 4094, 4095, 4096]]))
+    nph = nph.astype(np.int32)
+    nr = len(nph)
+    theta = np.linspace(0.3, np.pi / 2 - 0.02, nr)
+    ofs = np.concatenate([[0], np.cumsum(nph)[:-1]])
+    st = np.ones(nr, np.int32)
+    phi0 = np.linspace(0.0, 0.9, nr)
+    w = np.linspace(0.5, 1.5, nr) * 4 * np.pi / nph.sum()
+    g1 = sb.Geometry.general(nph, ofs, st, phi0, theta, w)
+    g2 = ref.general(nph, ofs, st, phi0, theta, w)
+    lmax = 2100
+    a1, a2 = sb.AlmInfo.triangular(lmax), ref.triangular(lmax, lmax)
+    npix = int(nph.sum())
+    na = _nalm(1, spin)
+    alms = [uniform_alm(lmax, seed=70 + i, spin=spin) for i in range(na)]
+    m1 = [np.zeros(npix) for _ in range(na)]
+    m2 = [np.zeros(npix) for _ in range(na)]
+    sb.execute(1, spin, [x.copy() for x in alms], m1, g1, a1, 1, DP)
+    ref.execute(1, spin, [x.copy() for x in alms], m2, g2, a2, 1, DP)
+    for x, y in zip(m1, m2):
+        assert rel_l2(x, y) < TOL
+    rng = np.random.default_rng(31 + spin)
+    maps = [rng.standard_normal(npix) for _ in range(na)]
+    b1 = [np.zeros(sb.nalm_triangular(lmax), np.complex128) for _ in range(na)]
+    b2 = [x.copy() for x in b1]
+    sb.execute(0, spin, b1, [x.copy() for x in maps], g1, a1, 1, DP)
+    ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, DP)
+    for x, y in zip(b1, b2):
+        assert rel_l2(x, y) < TOL
