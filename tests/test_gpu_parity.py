@@ -656,3 +656,59 @@ def test_ring_lengths_with_folding_at_high_lmax(ref, spin):
     ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, DP)
     for x, y in zip(b1, b2):
         assert rel_l2(x, y) < TOL
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_negative_and_interleaved_strides_match_reference(ref, spin):
+    # rings stored backwards (stride -1) and interleaved pairs (strides +2 and
+    # -2 over one pixel range), for a short ring, a folded mid-length ring,
+    # a 4096-pixel ring (which then leaves the power-of-two class for the
+    # register Bluestein one) and an 8188-pixel polar-style ring; both
+    # directions at 1e-12
+    specs = [(30, 1), (30, -1), (1000, -1), (4096, -1), (4096, 1), (8188, -1), (518, 2), (518, -2)]
+    nph = np.array([n for n, _ in specs], np.int32)
+    st = np.array([s for _, s in specs], np.int32)
+    ofs = np.zeros(len(specs), np.intp)
+    pos = 0
+    i = 0
+    while i < len(specs):
+        n, s = specs[i]
+        if abs(s) == 2:
+            # this ring and the next share 2n pixels: +2 from pos, -2 from the end
+            ofs[i] = pos
+            ofs[i + 1] = pos + 2 * n - 1
+            pos += 2 * n
+            i += 2
+            continue
+        ofs[i] = pos if s > 0 else pos + n - 1
+        pos += n
+        i += 1
+    npix = int(pos)
+    cover = np.zeros(npix, int)
+    for k in range(len(specs)):
+        cover[ofs[k] + st[k] * np.arange(nph[k])] += 1
+    assert cover.min() == 1 and cover.max() == 1
+    nr = len(specs)
+    theta = np.linspace(0.25, 1.45, nr)
+    phi0 = np.linspace(0.0, 0.6, nr)
+    w = np.linspace(0.5, 1.5, nr)
+    g1 = sb.Geometry.general(nph, ofs, st, phi0, theta, w)
+    g2 = ref.general(nph, ofs, st, phi0, theta, w)
+    lmax = 700
+    a1, a2 = sb.AlmInfo.triangular(lmax), ref.triangular(lmax, lmax)
+    na = _nalm(1, spin)
+    alms = [uniform_alm(lmax, seed=80 + i, spin=spin) for i in range(na)]
+    m1 = [np.zeros(npix) for _ in range(na)]
+    m2 = [np.zeros(npix) for _ in range(na)]
+    sb.execute(1, spin, [x.copy() for x in alms], m1, g1, a1, 1, DP)
+    ref.execute(1, spin, [x.copy() for x in alms], m2, g2, a2, 1, DP)
+    for x, y in zip(m1, m2):
+        assert rel_l2(x, y) < TOL
+    rng = np.random.default_rng(41 + spin)
+    maps = [rng.standard_normal(npix) for _ in range(na)]
+    b1 = [np.zeros(sb.nalm_triangular(lmax), np.complex128) for _ in range(na)]
+    b2 = [x.copy() for x in b1]
+    sb.execute(0, spin, b1, [x.copy() for x in maps], g1, a1, 1, DP)
+    ref.execute(0, spin, b2, [x.copy() for x in maps], g2, a2, 1, DP)
+    for x, y in zip(b1, b2):
+        assert rel_l2(x, y) < TOL
