@@ -657,7 +657,7 @@ def roofline(dom, dom_ms, dom_n, ops, B, steps, peak):
         values = ops[job[0]] / ((12 + 16 * B) if spin2 else (4 + 4 * B))
         flops_step = values * (12 if spin2 else 5) * dom_n / steps
         what = "mixed-kernel producer FP64 work (recurrence + quantisation), all launches of a step"
-        # the algorithmic count of the survey (reference opcnt of the whole
+        # the algorithmic count (the reference's opcnt of the whole
         # B-transform job, F_leg = triples (12 + 16 B) at spin s, (4 + 4 B) at 0)
         leg = ops[job[0]] / (dom_ms * 1e-3 / steps) / 1e12
     else:

@@ -1,8 +1,8 @@
 """GPU parity: the CUDA engine, called through the C ABI, against the
 reference libsharp (oracle/_ref) and the committed golden values.
 
-Tolerances: FP64 paths within 1e-12 relative L2 of the reference (the
-north-star bar); single-precision I/O within 1e-6; the reference test
+Tolerances: FP64 paths within 1e-12 relative L2 of the reference;
+single-precision I/O within 1e-6; the reference test
 suite's own known answers at its own tolerances (1e-12 / 1e-11)."""
 import json
 import math
