@@ -487,7 +487,10 @@ def run_ours(args, world, rank, local, clk, np, torch, sb):
     except ImportError:
         avail = 0
     need = B * 3 * (npix * 8 + 2 * nalm * 16)
-    nh = B if avail > 4 * need else 1   # distinct host buffers when host memory allows
+    # distinct host buffers when host memory allows (the ranks of this node
+    # allocate theirs at the same time)
+    local_world = max(1, int(os.environ.get("LOCAL_WORLD_SIZE", str(world))))
+    nh = B if avail > 4 * need * local_world else 1
     h_alm = [[pinned(nalm, torch.complex128) for _ in range(3)] for _ in range(nh)]
     h_map = [[pinned(npix, torch.float64) for _ in range(3)] for _ in range(nh)]
     h_out = [[pinned(nalm, torch.complex128) for _ in range(3)] for _ in range(nh)]
